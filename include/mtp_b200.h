@@ -1,0 +1,213 @@
+/*
+ * mtp_b200.h - C ABI of the B200 Moment Tensor Potential engine.
+ *
+ * This library replaces the reference's compiled-XLA bridge
+ * (pair_style_files/zero_overhead.{hpp,cpp}: a CPython/NumPy singleton that
+ * deserialises a jax.export executable and calls it every MD step) with
+ * hand-written sm_100a CUDA kernels behind plain C functions.  No torch,
+ * CPython or C++ types cross this boundary: pointers, sizes and int status
+ * codes only.  No C++ exception escapes any function.
+ *
+ * Conventions (identical to the reference evaluator jax_backend.py):
+ *   - a neighbour slot of centre atom i holds r_ij = x_j - x_i, the owner
+ *     index j of the neighbour, and its species t_j; a slot contributes
+ *     when t_j >= 0 and |r_ij| < max_dist of the potential
+ *     (jax_backend.py:83-90);
+ *   - slots whose owner index j is outside [0, natoms) still contribute to
+ *     E_i but their reaction force is dropped (jax_backend.py:292-299);
+ *   - forces F_k = sum_s dE_k/dr_ks - sum_{(i,s): j_is = k} dE_i/dr_is
+ *     (jax_backend.py:263-303);
+ *   - species are 0-based (LAMMPS type - 1, pair_jax_mtp.cpp:97).
+ *
+ * Virial conventions:
+ *   - mtp_compute*: LAMMPS virial in energy units, W = -sum r (x) dE/dr,
+ *     symmetrised, order xx, yy, zz, xy, xz, yz (what Pair::virial holds);
+ *   - mtp_execute_potential: the reference's `stress` output unchanged,
+ *     sym(sum r (x) dE/dr) / V in order xx, yy, zz, yz, xz, xy
+ *     (jax_backend.py:355-360, consumed at pair_jax_mtp.cpp:203-205).
+ *
+ * Thread safety: a handle is used by one host thread at a time.  Each handle
+ * owns its device buffers and one CUDA stream (settable).
+ */
+#ifndef MTP_B200_H
+#define MTP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MTP_B200_ABI_VERSION 1
+
+/* Status codes returned by every entry point. */
+typedef enum mtp_status {
+  MTP_OK = 0,
+  MTP_E_INVALID = 1,    /* bad argument (null pointer, negative size, ...)          */
+  MTP_E_FORMAT = 2,     /* malformed .mtp file or unsupported table structure       */
+  MTP_E_CAPACITY = 3,   /* natoms > max_atoms or a row longer than max_nbr          */
+  MTP_E_SPECIES = 4,    /* a species index outside [0, species_count)               */
+  MTP_E_NONFINITE = 5,  /* NaN/Inf produced on the device                           */
+  MTP_E_CUDA = 6,       /* CUDA runtime error (text in mtp_last_error)              */
+  MTP_E_NODEVICE = 7,   /* no usable CUDA device                                    */
+  MTP_E_OOM = 8         /* device allocation failed                                 */
+} mtp_status;
+
+/* Arithmetic of the evaluator. */
+typedef enum mtp_precision {
+  MTP_PRECISION_FP64 = 0,   /* everything in FP64 (the drop-in)                       */
+  MTP_PRECISION_MIXED = 1   /* FP32 radial/moments/contractions; FP64 energy, virial,
+                               force accumulation                                      */
+} mtp_precision;
+
+/* Output selection flags for mtp_compute*. */
+#define MTP_EFLAG 1   /* total energy           */
+#define MTP_VFLAG 2   /* global virial          */
+#define MTP_EATOM 4   /* per-atom energies      */
+#define MTP_VATOM 8   /* per-atom virial        */
+#define MTP_REUSE_NEIGHBORS 16  /* mtp_compute_device: the neighbour indices are those of the
+                                   previous call; skip rebuilding the incoming-slot lists  */
+
+typedef struct mtp_handle mtp_handle;
+
+/* Library ABI version (MTP_B200_ABI_VERSION of the build). */
+int mtp_abi_version(void);
+
+/*
+ * Create an evaluator from an .mtp potential file.
+ * Replaces PairJaxMTP::settings + init_style + ZeroOverheadContext
+ * (pair_jax_mtp.cpp:228-245, 264-282; zero_overhead.cpp:159-169, 317-320):
+ * max_atoms and max_nbr are the pair style's MAX_ATOMS and
+ * MAX_ATOMS_PER_NEIGHBOR capacities, cutoff its MTP_CUTOFF, debug_level its
+ * DEBUG_LEVEL (0 silent, 1 summary at destroy, 2 per-call timing to stderr).
+ * The reference takes a .bin export here; a path ending in ".bin" is
+ * rejected with MTP_E_FORMAT.
+ */
+int mtp_create(const char* mtp_path, int max_atoms, int max_nbr, double cutoff, int debug_level,
+               int precision, mtp_handle** out);
+
+/* Release every device buffer of the handle. */
+void mtp_destroy(mtp_handle* h);
+
+/* Text of the last error on this handle (or of the last failed mtp_create when h is NULL). */
+const char* mtp_last_error(const mtp_handle* h);
+
+/* Use this CUDA stream (a cudaStream_t) for all work of the handle; NULL = the handle's own. */
+int mtp_set_stream(mtp_handle* h, void* cuda_stream);
+
+/* Basis sizes of the loaded potential: out[0..7] = species_count, radial_funcs_count,
+ * radial_basis_size, alpha_moments_count, alpha_index_basic_count,
+ * alpha_index_times_count, alpha_scalar_moments, max monomial degree. */
+int mtp_get_info(const mtp_handle* h, int* out8);
+
+/* Replace the coefficients (training updates): species [S], moment [Sa], radial [S*S*R*K]
+ * in .mtp order.  Any pointer may be NULL to keep the current values. */
+int mtp_set_coeffs(mtp_handle* h, const double* species_coeffs, const double* moment_coeffs,
+                   const double* radial_coeffs);
+
+/*
+ * Drop-in for ZeroOverheadManager::execute_potential (zero_overhead.hpp:58-64,
+ * zero_overhead.cpp:171-272), same arguments and meaning: per-atom row
+ * pointers of r_ij (3 doubles per neighbour), neighbour owner indices and
+ * neighbour species, neighbour counts, cell volume.  Outputs the total energy,
+ * forces[i][0..2] for i < natoms, and stress[6] in the reference's convention
+ * (see above).  Returns MTP_OK (the reference returned bool true) or an error.
+ */
+int mtp_execute_potential(mtp_handle* h, int natoms, int nneigh_total,
+                          const double* const* atom_positions, const int* atom_types,
+                          const int* const* neighbor_lists, const int* neighbor_counts,
+                          const int* const* neighbor_types_lists, double volume,
+                          double* energy, double** forces, double* stress);
+
+/*
+ * Flat host-buffer evaluation (the pair style's fast path).
+ * itypes [natoms]; rijs [natoms][nbr_stride][3]; js, jtypes [natoms][nbr_stride];
+ * counts [natoms] (NULL: every slot of a row is examined, empty slots have
+ * jtype < 0).  nbr_stride <= max_nbr.  Outputs selected by flags; pointers of
+ * unselected outputs may be NULL.  forces [natoms][3] is always written.
+ * virial [6] (LAMMPS order), eatom [natoms], vatom [natoms][6].
+ * Synchronous: returns when results are in host memory.
+ */
+int mtp_compute(mtp_handle* h, int natoms, int nbr_stride, const int* itypes, const double* rijs,
+                const int* js, const int* jtypes, const int* counts, int flags, double* energy,
+                double* forces, double* virial, double* eatom, double* vatom);
+
+/*
+ * Device-pointer variant of mtp_compute for PyTorch and CUDA-graph capture:
+ * every pointer is device memory; work is enqueued on the handle's stream and
+ * the call returns without synchronising.  energy [1], virial [6].
+ * Device-side error flags are read with mtp_sync_status.
+ */
+int mtp_compute_device(mtp_handle* h, int natoms, int nbr_stride, const int* d_itypes,
+                       const double* d_rijs, const int* d_js, const int* d_jtypes,
+                       const int* d_counts, int flags, double* d_energy, double* d_forces,
+                       double* d_virial, double* d_eatom, double* d_vatom);
+
+/* Synchronise the handle's stream and report device-side error flags
+ * (MTP_E_NONFINITE, MTP_E_SPECIES) raised since the last call. */
+int mtp_sync_status(mtp_handle* h);
+
+/*
+ * Batched evaluation of many configurations in one launch (training
+ * forward).  Atoms of all configurations are concatenated; js holds global
+ * atom indices; cfg_of_atom [natoms] maps atoms to configurations
+ * [0, nconfig).  Outputs (device): energy [nconfig], forces [natoms][3],
+ * stress [nconfig][6] in the reference's convention (sym(sum r g)/V, order
+ * xx,yy,zz,yz,xz,xy) using volumes [nconfig] (device), as the reference
+ * training code computes it (motep_original_files/jax_engine/jax.py:76-91).
+ */
+int mtp_compute_batch_device(mtp_handle* h, int natoms, int nbr_stride, int nconfig,
+                             const int* d_itypes, const double* d_rijs, const int* d_js,
+                             const int* d_jtypes, const int* d_counts, const int* d_cfg_of_atom,
+                             const double* d_volumes, double* d_energy, double* d_forces,
+                             double* d_stress);
+
+/*
+ * Adjoint of mtp_compute_batch_device with respect to the coefficients
+ * (the gradient jax.grad takes of the training loss,
+ * training/motep_jax_train_function.py:67-87, 191).  Given upstream
+ * gradients gE [nconfig], gF [natoms][3], gS [nconfig][6] (device) for the
+ * same inputs, writes (device) dL/d species_coeffs [S], dL/d moment_coeffs
+ * [Sa] and dL/d radial_coeffs [S*S*R*K].  Second derivatives of the forces
+ * and stress are included.  Deterministic.
+ */
+int mtp_adjoint_batch_device(mtp_handle* h, int natoms, int nbr_stride, int nconfig,
+                             const int* d_itypes, const double* d_rijs, const int* d_js,
+                             const int* d_jtypes, const int* d_counts, const int* d_cfg_of_atom,
+                             const double* d_volumes, const double* d_gE, const double* d_gF,
+                             const double* d_gS, double* d_gspecies, double* d_gmoment,
+                             double* d_gradial);
+
+/* Launch shape of the evaluation kernel: threads per block (128/256/512) and
+ * blocks per SM (0 = as many as fit).  Used by the autotuner. */
+int mtp_set_launch(mtp_handle* h, int threads_per_block, int blocks_per_sm);
+
+/* Last evaluation kernel's launch: out4 = threads, blocks, dynamic shared bytes, blocks per SM. */
+int mtp_get_launch(const mtp_handle* h, int* out4);
+
+/*
+ * Parse an .mtp file on the host only (no device needed) and report its
+ * basis sizes in the layout of mtp_get_info.  Used to validate files.
+ */
+int mtp_parse_info(const char* mtp_path, int* out8, char* err, int err_len);
+
+/*
+ * Host execution of the contraction schedule for one atom (no device needed;
+ * a test hook for the table preprocessing).  basic [alpha_index_basic_count]
+ * moments in, moments [alpha_moments_count] and dE/dmoment [alpha_moments_count]
+ * out, using the handle-free preprocessing of the file and the schedule for
+ * threads_per_block lanes.
+ */
+int mtp_schedule_emulate(const char* mtp_path, int threads_per_block, const double* basic,
+                         double* moments, double* dmoments, double* energy_part);
+
+/* Peak FP64 / FP32 FMA throughput of device 0 measured by an FMA-chain kernel
+ * (TFLOP/s, an FMA counted as 2 flops).  Used for the roofline. */
+int mtp_measure_fma_peak(double* fp64_tflops, double* fp32_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MTP_B200_H */

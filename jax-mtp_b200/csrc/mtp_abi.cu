@@ -1,0 +1,688 @@
+// mtp_abi.cu - the C ABI (include/mtp_b200.h): handles, device buffers, calls.
+//
+// Replaces the reference bridge pair_style_files/zero_overhead.cpp: instead
+// of refilling NumPy buffers with sentinels and calling a deserialised JAX
+// executable through CPython every step (zero_overhead.cpp:61-117, 171-272),
+// a handle owns device buffers sized by the pair style's capacities and
+// launches the sm_100a kernels directly.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mtp_b200.h"
+#include "mtp_launch.hpp"
+#include "mtp_model.hpp"
+#include "mtp_train.hpp"
+
+using namespace mtp;
+
+namespace {
+
+std::string g_create_error;
+
+struct DeviceSchedule {
+  Schedule sched;
+  uint2* d_entries = nullptr;
+};
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  return cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+}
+
+}  // namespace
+
+struct mtp_handle {
+  Potential pot;
+  int max_atoms = 0, max_nbr = 0, debug = 0, precision = 0;
+  double cutoff = 0.0;
+  int device = 0, sm_count = 0;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  int threads = 256, blocks_per_sm = 0;
+  int last_threads = 0, last_blocks = 0, last_bps = 0;
+  bool last_vglobal = false;
+  void* d_vscratch = nullptr;
+  size_t vscratch_bytes = 0;
+  size_t last_smem = 0;
+  std::map<int, DeviceSchedule> scheds;
+  // potential tables on the device
+  double *d_radial = nullptr, *d_species = nullptr, *d_theta = nullptr, *d_seed_val = nullptr;
+  int *d_mapping = nullptr, *d_seed_idx = nullptr, *d_zero = nullptr, *d_abc = nullptr, *d_mk = nullptr;
+  int nseed = 0;
+  // input / output / scratch buffers sized by the capacities
+  int *d_itypes = nullptr, *d_js = nullptr, *d_jtypes = nullptr, *d_counts = nullptr;
+  double* d_rijs = nullptr;
+  double *d_G = nullptr, *d_E = nullptr, *d_F = nullptr, *d_wown = nullptr, *d_vatom = nullptr;
+  int *d_in_cnt = nullptr, *d_in_ptr = nullptr, *d_in_cursor = nullptr, *d_in_slot = nullptr, *d_blk = nullptr;
+  double *d_partials = nullptr, *d_tot = nullptr;
+  int* d_err = nullptr;
+  int* d_cfg_ptr = nullptr;
+  int cfg_cap = 0;
+  double* h_tot = nullptr;   // pinned [7]
+  int* h_err = nullptr;      // pinned [1]
+  TrainWorkspace train;
+  // statistics
+  long long calls = 0;
+  double total_ms = 0.0;
+  std::string err;
+};
+
+namespace {
+
+int fail(mtp_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+int cuda_fail(mtp_handle* h, cudaError_t e, const char* what) {
+  return fail(h, MTP_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define MTP_CUDA(h, call)                                  \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return cuda_fail((h), e_, #call); \
+  } while (0)
+
+DevModel make_model(mtp_handle* h, const DeviceSchedule& ds) {
+  DevModel md{};
+  const Schedule& s = ds.sched;
+  md.entries = ds.d_entries;
+  md.nfwd = static_cast<int>(s.fwd.size());
+  md.nrev = static_cast<int>(s.rev.size());
+  for (int i = 0; i < md.nfwd; ++i) md.fwd[i] = DevPass{s.fwd[i].offset, s.fwd[i].steps};
+  for (int i = 0; i < md.nrev; ++i) md.rev[i] = DevPass{s.rev[i].offset, s.rev[i].steps};
+  md.radial = h->d_radial;
+  md.species = h->d_species;
+  md.theta = h->d_theta;
+  md.mapping = h->d_mapping;
+  md.seed_idx = h->d_seed_idx;
+  md.seed_val = h->d_seed_val;
+  md.nseed = h->nseed;
+  md.zero_list = h->d_zero;
+  md.nzero = static_cast<int>(s.zero_list.size());
+  md.mono_abc = h->d_abc;
+  md.mono_k = h->d_mk;
+  md.S = h->pot.S;
+  md.R = h->pot.R;
+  md.K = h->pot.K;
+  md.M = h->pot.M;
+  md.B = h->pot.B;
+  md.P = s.P;
+  md.D = s.D;
+  md.Sa = h->pot.Sa;
+  md.v_m = s.v_m;
+  md.v_dm = s.v_dm;
+  md.v_zero = s.v_zero;
+  md.v_one = s.v_one;
+  md.v_size = s.v_size;
+  md.scaling = h->pot.scaling;
+  md.rmin = h->pot.min_dist;
+  md.rmax = h->pot.max_dist;
+  return md;
+}
+
+// Schedule for `lanes`, built and uploaded on first use.
+int get_schedule(mtp_handle* h, int lanes, DeviceSchedule** out) {
+  auto it = h->scheds.find(lanes);
+  if (it == h->scheds.end()) {
+    DeviceSchedule ds;
+    std::string err;
+    if (!build_schedule(h->pot, lanes, ds.sched, err)) return fail(h, MTP_E_FORMAT, err);
+    const auto& ent = ds.sched.entries;
+    MTP_CUDA(h, dalloc(&ds.d_entries, ent.size() / 2));
+    MTP_CUDA(h, cudaMemcpy(ds.d_entries, ent.data(), ent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if (h->d_abc == nullptr) {
+      MTP_CUDA(h, dalloc(&h->d_abc, ds.sched.mono_abc.size()));
+      MTP_CUDA(h, cudaMemcpy(h->d_abc, ds.sched.mono_abc.data(), ds.sched.mono_abc.size() * sizeof(int),
+                             cudaMemcpyHostToDevice));
+      MTP_CUDA(h, dalloc(&h->d_mk, ds.sched.mono_k.size()));
+      MTP_CUDA(h, cudaMemcpy(h->d_mk, ds.sched.mono_k.data(), ds.sched.mono_k.size() * sizeof(int),
+                             cudaMemcpyHostToDevice));
+      MTP_CUDA(h, dalloc(&h->d_zero, ds.sched.zero_list.size()));
+      if (!ds.sched.zero_list.empty())
+        MTP_CUDA(h, cudaMemcpy(h->d_zero, ds.sched.zero_list.data(), ds.sched.zero_list.size() * sizeof(int),
+                               cudaMemcpyHostToDevice));
+    }
+    it = h->scheds.emplace(lanes, ds).first;
+  }
+  *out = &it->second;
+  return MTP_OK;
+}
+
+int upload_coeffs(mtp_handle* h) {
+  const Potential& p = h->pot;
+  MTP_CUDA(h, cudaMemcpy(h->d_radial, p.radial.data(), p.radial.size() * sizeof(double), cudaMemcpyHostToDevice));
+  MTP_CUDA(h, cudaMemcpy(h->d_species, p.species.data(), p.species.size() * sizeof(double), cudaMemcpyHostToDevice));
+  MTP_CUDA(h, cudaMemcpy(h->d_theta, p.moment.data(), p.moment.size() * sizeof(double), cudaMemcpyHostToDevice));
+  std::vector<int> si;
+  std::vector<double> sv;
+  seed_list(p, si, sv);
+  h->nseed = static_cast<int>(si.size());
+  MTP_CUDA(h, cudaMemcpy(h->d_seed_idx, si.data(), si.size() * sizeof(int), cudaMemcpyHostToDevice));
+  MTP_CUDA(h, cudaMemcpy(h->d_seed_val, sv.data(), sv.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return MTP_OK;
+}
+
+void free_handle(mtp_handle* h) {
+  if (!h) return;
+  auto F = [](void* p) { if (p) cudaFree(p); };
+  for (auto& kv : h->scheds) F(kv.second.d_entries);
+  F(h->d_radial); F(h->d_species); F(h->d_theta); F(h->d_seed_val);
+  F(h->d_mapping); F(h->d_seed_idx); F(h->d_zero); F(h->d_abc); F(h->d_mk);
+  F(h->d_itypes); F(h->d_js); F(h->d_jtypes); F(h->d_counts); F(h->d_rijs);
+  F(h->d_G); F(h->d_E); F(h->d_F); F(h->d_wown); F(h->d_vatom);
+  F(h->d_in_cnt); F(h->d_in_ptr); F(h->d_in_cursor); F(h->d_in_slot); F(h->d_blk);
+  F(h->d_partials); F(h->d_tot); F(h->d_err); F(h->d_cfg_ptr); F(h->d_vscratch);
+  train_free(h->train);
+  if (h->h_tot) cudaFreeHost(h->h_tot);
+  if (h->h_err) cudaFreeHost(h->h_err);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+}
+
+// Launch shape for the evaluation kernel at the current settings: the
+// requested lanes with the value space in shared memory, else fewer lanes,
+// else the value space in global memory.
+int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, int* blocks_out, bool fp64,
+                bool* vglobal_out) {
+  int lanes = h->threads;
+  DeviceSchedule* ds = nullptr;
+  bool vglobal = false;
+  int bps = 0;
+  for (int alt : {lanes, 256, 128}) {
+    if (alt > lanes) continue;
+    int st = get_schedule(h, alt, &ds);
+    if (st != MTP_OK) return st;
+    bps = eval_blocks_per_sm(make_model(h, *ds), stride, alt, fp64, false);
+    if (bps > 0) {
+      lanes = alt;
+      break;
+    }
+  }
+  if (bps <= 0) {
+    lanes = h->threads;
+    int st = get_schedule(h, lanes, &ds);
+    if (st != MTP_OK) return st;
+    vglobal = true;
+    bps = eval_blocks_per_sm(make_model(h, *ds), stride, lanes, fp64, true);
+  }
+  if (bps <= 0)
+    return fail(h, MTP_E_CAPACITY, "the evaluation block does not fit in shared memory for this basis and max_nbr");
+  if (h->blocks_per_sm > 0) bps = std::min(bps, h->blocks_per_sm);
+  long long blocks = static_cast<long long>(bps) * h->sm_count;
+  blocks = std::max(1LL, std::min<long long>(blocks, natoms));
+  if (vglobal) {
+    const size_t need = static_cast<size_t>(blocks) * ds->sched.v_size * (fp64 ? sizeof(double) : sizeof(float));
+    if (need > h->vscratch_bytes) {
+      if (h->d_vscratch) cudaFree(h->d_vscratch);
+      h->d_vscratch = nullptr;
+      h->vscratch_bytes = 0;
+      MTP_CUDA(h, cudaMalloc(&h->d_vscratch, need));
+      h->vscratch_bytes = need;
+    }
+  }
+  *ds_out = ds;
+  *blocks_out = static_cast<int>(blocks);
+  *vglobal_out = vglobal;
+  h->last_threads = lanes;
+  h->last_blocks = static_cast<int>(blocks);
+  h->last_bps = bps;
+  h->last_vglobal = vglobal;
+  h->last_smem = eval_smem_bytes(make_model(h, *ds), stride, lanes, fp64, vglobal);
+  return MTP_OK;
+}
+
+// Evaluate site energies and per-slot gradients, then forces and virials.
+int run_device(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
+               const int* jtypes, const int* counts, bool rebuild_incoming, double* forces, double* vatom) {
+  const bool fp64 = h->precision == MTP_PRECISION_FP64;
+  DeviceSchedule* ds = nullptr;
+  int blocks = 0;
+  bool vglobal = false;
+  int st = pick_launch(h, natoms, stride, &ds, &blocks, fp64, &vglobal);
+  if (st != MTP_OK) return st;
+  DevModel md = make_model(h, *ds);
+  DevIO io{};
+  io.natoms = natoms;
+  io.nbr_stride = stride;
+  io.n_pad = stride;
+  io.itypes = itypes;
+  io.rijs = rijs;
+  io.jtypes = jtypes;
+  io.counts = counts;
+  io.site_energy = h->d_E;
+  io.pair_grad = h->d_G;
+  io.err = h->d_err;
+  io.vscratch = h->d_vscratch;
+  if (rebuild_incoming) {
+    MTP_CUDA(h, launch_incoming(natoms, stride, js, jtypes, counts, h->d_in_cnt, h->d_in_ptr, h->d_in_cursor,
+                                h->d_in_slot, h->d_blk, h->stream));
+  }
+  MTP_CUDA(h, launch_eval(md, io, h->last_threads, blocks, fp64, vglobal, h->stream));
+  MTP_CUDA(h, launch_force_gather(natoms, stride, rijs, counts, h->d_G, h->d_in_ptr, h->d_in_slot, forces,
+                                  h->d_wown, vatom, h->stream));
+  return MTP_OK;
+}
+
+int read_err_flags(mtp_handle* h) {
+  MTP_CUDA(h, cudaMemcpyAsync(h->h_err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  MTP_CUDA(h, cudaStreamSynchronize(h->stream));
+  int f = *h->h_err;
+  if (f) MTP_CUDA(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+  if (f & kErrSpecies) return fail(h, MTP_E_SPECIES, "a species index is outside [0, species_count)");
+  if (f & kErrCapacity) return fail(h, MTP_E_CAPACITY, "a neighbour count exceeds the row length");
+  if (f & kErrNonFinite) return fail(h, MTP_E_NONFINITE, "non-finite energy or force produced on the device");
+  return MTP_OK;
+}
+
+bool ends_with(const std::string& s, const std::string& suf) {
+  return s.size() >= suf.size() && s.compare(s.size() - suf.size(), suf.size(), suf) == 0;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int mtp_abi_version(void) { return MTP_B200_ABI_VERSION; }
+
+int mtp_parse_info(const char* path, int* out8, char* errbuf, int err_len) {
+  if (!path || !out8) return MTP_E_INVALID;
+  Potential pot;
+  std::string err;
+  if (!parse_mtp_file(path, pot, err)) {
+    if (errbuf && err_len > 0) std::snprintf(errbuf, err_len, "%s", err.c_str());
+    return MTP_E_FORMAT;
+  }
+  int D = 0;
+  for (int k = 0; k < pot.B; ++k) D = std::max(D, pot.basic[4 * k + 1] + pot.basic[4 * k + 2] + pot.basic[4 * k + 3]);
+  const int v[8] = {pot.S, pot.R, pot.K, pot.M, pot.B, pot.T, pot.Sa, D};
+  std::memcpy(out8, v, sizeof(v));
+  return MTP_OK;
+}
+
+int mtp_schedule_emulate(const char* path, int lanes, const double* basic, double* moments, double* dmoments,
+                         double* energy_part) {
+  if (!path || !basic || !moments || !dmoments) return MTP_E_INVALID;
+  Potential pot;
+  std::string err;
+  if (!parse_mtp_file(path, pot, err)) return MTP_E_FORMAT;
+  Schedule s;
+  if (!build_schedule(pot, lanes, s, err)) return MTP_E_FORMAT;
+  std::vector<double> V(s.v_size, 0.0);
+  for (int k = 0; k < pot.B; ++k) V[s.v_m + k] = basic[k];
+  double e = emulate_schedule(pot, s, V);
+  for (int k = 0; k < pot.M; ++k) {
+    moments[k] = V[s.v_m + k];
+    dmoments[k] = V[s.v_dm + k];
+  }
+  if (energy_part) *energy_part = e;
+  return MTP_OK;
+}
+
+int mtp_create(const char* mtp_path, int max_atoms, int max_nbr, double cutoff, int debug_level, int precision,
+               mtp_handle** out) {
+  if (!out) return fail(nullptr, MTP_E_INVALID, "out is null");
+  *out = nullptr;
+  if (!mtp_path) return fail(nullptr, MTP_E_INVALID, "mtp_path is null");
+  if (max_atoms <= 0 || max_nbr <= 0 || !(cutoff > 0.0))
+    return fail(nullptr, MTP_E_INVALID, "max_atoms, max_nbr and cutoff must be positive");
+  if (precision != MTP_PRECISION_FP64 && precision != MTP_PRECISION_MIXED)
+    return fail(nullptr, MTP_E_INVALID, "precision must be MTP_PRECISION_FP64 or MTP_PRECISION_MIXED");
+  if (max_nbr > 1024) return fail(nullptr, MTP_E_CAPACITY, "max_nbr above the supported 1024");
+  if (static_cast<long long>(max_atoms) * max_nbr >= (1LL << 31))
+    return fail(nullptr, MTP_E_CAPACITY, "max_atoms * max_nbr must stay below 2^31");
+  std::string path(mtp_path);
+  if (ends_with(path, ".bin"))
+    return fail(nullptr, MTP_E_FORMAT,
+                "'" + path + "' looks like a jax.export .bin; this engine reads the .mtp potential file itself");
+  auto* h = new mtp_handle();
+  h->max_atoms = max_atoms;
+  h->max_nbr = max_nbr;
+  h->cutoff = cutoff;
+  h->debug = debug_level;
+  h->precision = precision;
+  std::string err;
+  if (!parse_mtp_file(path, h->pot, err)) {
+    delete h;
+    return fail(nullptr, MTP_E_FORMAT, err);
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    delete h;
+    return fail(nullptr, MTP_E_NODEVICE, "no CUDA device");
+  }
+  auto bail = [&](int code) {
+    g_create_error = h->err;
+    free_handle(h);
+    return code;
+  };
+  if (cudaGetDevice(&h->device) != cudaSuccess) return bail(cuda_fail(h, cudaGetLastError(), "cudaGetDevice"));
+  cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device);
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(cuda_fail(h, cudaGetLastError(), "cudaStreamCreate"));
+  h->stream = h->own_stream;
+  const Potential& p = h->pot;
+  const size_t N = static_cast<size_t>(max_atoms), NS = N * max_nbr;
+  bool ok = dalloc(&h->d_radial, p.radial.size()) == cudaSuccess && dalloc(&h->d_species, p.S) == cudaSuccess &&
+            dalloc(&h->d_theta, p.Sa) == cudaSuccess && dalloc(&h->d_mapping, p.Sa) == cudaSuccess &&
+            dalloc(&h->d_seed_idx, p.Sa) == cudaSuccess && dalloc(&h->d_seed_val, p.Sa) == cudaSuccess &&
+            dalloc(&h->d_itypes, N) == cudaSuccess && dalloc(&h->d_js, NS) == cudaSuccess &&
+            dalloc(&h->d_jtypes, NS) == cudaSuccess && dalloc(&h->d_counts, N) == cudaSuccess &&
+            dalloc(&h->d_rijs, 3 * NS) == cudaSuccess && dalloc(&h->d_G, 3 * NS) == cudaSuccess &&
+            dalloc(&h->d_E, N) == cudaSuccess && dalloc(&h->d_F, 3 * N) == cudaSuccess &&
+            dalloc(&h->d_wown, 6 * N) == cudaSuccess && dalloc(&h->d_vatom, 6 * N) == cudaSuccess &&
+            dalloc(&h->d_in_cnt, N) == cudaSuccess && dalloc(&h->d_in_ptr, N + 1) == cudaSuccess &&
+            dalloc(&h->d_in_cursor, N) == cudaSuccess && dalloc(&h->d_in_slot, NS) == cudaSuccess &&
+            dalloc(&h->d_blk, (N + 1023) / 1024 + 1) == cudaSuccess &&
+            dalloc(&h->d_partials, 7 * kReduceBlocks) == cudaSuccess && dalloc(&h->d_tot, 8) == cudaSuccess &&
+            dalloc(&h->d_err, 1) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    h->err = "device allocation failed for the requested capacities";
+    return bail(MTP_E_OOM);
+  }
+  if (cudaMallocHost(&h->h_tot, 8 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&h->h_err, sizeof(int)) != cudaSuccess) {
+    h->err = "pinned host allocation failed";
+    return bail(MTP_E_OOM);
+  }
+  cudaMemset(h->d_err, 0, sizeof(int));
+  if (cudaMemcpy(h->d_mapping, p.mapping.data(), p.Sa * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(cuda_fail(h, cudaGetLastError(), "upload mapping"));
+  int st = upload_coeffs(h);
+  if (st != MTP_OK) return bail(st);
+  DeviceSchedule* ds = nullptr;
+  st = get_schedule(h, h->threads, &ds);
+  if (st != MTP_OK) return bail(st);
+  if (h->debug >= 1) {
+    std::fprintf(stderr, "[mtp_b200] %s: S=%d R=%d K=%d M=%d B=%d T=%d Sa=%d; %d fwd + %d rev passes, %d value slots\n",
+                 path.c_str(), p.S, p.R, p.K, p.M, p.B, p.T, p.Sa, static_cast<int>(ds->sched.fwd.size()),
+                 static_cast<int>(ds->sched.rev.size()), ds->sched.v_size);
+  }
+  *out = h;
+  return MTP_OK;
+}
+
+void mtp_destroy(mtp_handle* h) {
+  if (!h) return;
+  if (h->debug >= 1 && h->calls > 0)
+    std::fprintf(stderr, "[mtp_b200] %lld calls, %.3f ms total, %.3f ms/call\n", h->calls, h->total_ms,
+                 h->total_ms / h->calls);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_handle(h);
+}
+
+const char* mtp_last_error(const mtp_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int mtp_set_stream(mtp_handle* h, void* s) {
+  if (!h) return MTP_E_INVALID;
+  h->stream = s ? static_cast<cudaStream_t>(s) : h->own_stream;
+  return MTP_OK;
+}
+
+int mtp_get_info(const mtp_handle* h, int* out8) {
+  if (!h || !out8) return MTP_E_INVALID;
+  const Potential& p = h->pot;
+  int D = 0;
+  for (int k = 0; k < p.B; ++k) D = std::max(D, p.basic[4 * k + 1] + p.basic[4 * k + 2] + p.basic[4 * k + 3]);
+  const int v[8] = {p.S, p.R, p.K, p.M, p.B, p.T, p.Sa, D};
+  std::memcpy(out8, v, sizeof(v));
+  return MTP_OK;
+}
+
+int mtp_set_coeffs(mtp_handle* h, const double* species, const double* moment, const double* radial) {
+  if (!h) return MTP_E_INVALID;
+  Potential& p = h->pot;
+  if (species) std::copy(species, species + p.S, p.species.begin());
+  if (moment) std::copy(moment, moment + p.Sa, p.moment.begin());
+  if (radial) std::copy(radial, radial + p.radial.size(), p.radial.begin());
+  MTP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return upload_coeffs(h);
+}
+
+int mtp_set_launch(mtp_handle* h, int threads, int bps) {
+  if (!h) return MTP_E_INVALID;
+  if (threads != 64 && threads != 128 && threads != 256 && threads != 512)
+    return fail(h, MTP_E_INVALID, "threads_per_block must be 64, 128, 256 or 512");
+  h->threads = threads;
+  h->blocks_per_sm = std::max(0, bps);
+  return MTP_OK;
+}
+
+int mtp_get_launch(const mtp_handle* h, int* out4) {
+  if (!h || !out4) return MTP_E_INVALID;
+  out4[0] = h->last_threads;
+  out4[1] = h->last_blocks;
+  out4[2] = static_cast<int>(h->last_smem);
+  out4[3] = h->last_bps;
+  return MTP_OK;
+}
+
+int mtp_sync_status(mtp_handle* h) {
+  if (!h) return MTP_E_INVALID;
+  return read_err_flags(h);
+}
+
+int mtp_compute_device(mtp_handle* h, int natoms, int stride, const int* d_itypes, const double* d_rijs,
+                       const int* d_js, const int* d_jtypes, const int* d_counts, int flags, double* d_energy,
+                       double* d_forces, double* d_virial, double* d_eatom, double* d_vatom) {
+  if (!h) return MTP_E_INVALID;
+  if (natoms < 0 || stride <= 0) return fail(h, MTP_E_INVALID, "natoms must be >= 0 and nbr_stride > 0");
+  if (natoms > h->max_atoms) return fail(h, MTP_E_CAPACITY, "natoms exceeds max_atoms");
+  if (stride > h->max_nbr) return fail(h, MTP_E_CAPACITY, "nbr_stride exceeds max_nbr");
+  if (natoms > 0 && (!d_itypes || !d_rijs || !d_js || !d_jtypes || !d_forces))
+    return fail(h, MTP_E_INVALID, "null input or forces pointer");
+  if ((flags & MTP_EFLAG) && !d_energy) return fail(h, MTP_E_INVALID, "MTP_EFLAG without an energy pointer");
+  if ((flags & MTP_VFLAG) && !d_virial) return fail(h, MTP_E_INVALID, "MTP_VFLAG without a virial pointer");
+  if ((flags & MTP_EATOM) && !d_eatom) return fail(h, MTP_E_INVALID, "MTP_EATOM without an eatom pointer");
+  if ((flags & MTP_VATOM) && !d_vatom) return fail(h, MTP_E_INVALID, "MTP_VATOM without a vatom pointer");
+  const bool rebuild = !(flags & MTP_REUSE_NEIGHBORS);
+  int st = run_device(h, natoms, stride, d_itypes, d_rijs, d_js, d_jtypes, d_counts, rebuild, d_forces,
+                      (flags & MTP_VATOM) ? d_vatom : nullptr);
+  if (st != MTP_OK) return st;
+  if (flags & (MTP_EFLAG | MTP_VFLAG)) {
+    MTP_CUDA(h, launch_totals(natoms, h->d_E, h->d_wown, h->d_partials, h->d_tot, h->stream));
+    if (flags & MTP_EFLAG)
+      MTP_CUDA(h, cudaMemcpyAsync(d_energy, h->d_tot, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    if (flags & MTP_VFLAG)
+      MTP_CUDA(h, cudaMemcpyAsync(d_virial, h->d_tot + 1, 6 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  }
+  if ((flags & MTP_EATOM) && natoms > 0)
+    MTP_CUDA(h, cudaMemcpyAsync(d_eatom, h->d_E, natoms * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  h->calls++;
+  return MTP_OK;
+}
+
+int mtp_compute(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
+                const int* jtypes, const int* counts, int flags, double* energy, double* forces, double* virial,
+                double* eatom, double* vatom) {
+  if (!h) return MTP_E_INVALID;
+  if (natoms < 0 || stride <= 0) return fail(h, MTP_E_INVALID, "natoms must be >= 0 and nbr_stride > 0");
+  if (natoms > h->max_atoms)
+    return fail(h, MTP_E_CAPACITY, "natoms " + std::to_string(natoms) + " exceeds max_atoms " +
+                                        std::to_string(h->max_atoms));
+  if (stride > h->max_nbr) return fail(h, MTP_E_CAPACITY, "nbr_stride exceeds max_nbr");
+  if (natoms > 0 && (!itypes || !rijs || !js || !jtypes || !forces))
+    return fail(h, MTP_E_INVALID, "null input or forces pointer");
+  if ((flags & MTP_EFLAG) && !energy) return fail(h, MTP_E_INVALID, "MTP_EFLAG without an energy pointer");
+  if ((flags & MTP_VFLAG) && !virial) return fail(h, MTP_E_INVALID, "MTP_VFLAG without a virial pointer");
+  if ((flags & MTP_EATOM) && !eatom) return fail(h, MTP_E_INVALID, "MTP_EATOM without an eatom pointer");
+  if ((flags & MTP_VATOM) && !vatom) return fail(h, MTP_E_INVALID, "MTP_VATOM without a vatom pointer");
+  if (counts) {
+    for (int i = 0; i < natoms; ++i)
+      if (counts[i] < 0 || counts[i] > stride)
+        return fail(h, MTP_E_CAPACITY, "atom " + std::to_string(i) + " has " + std::to_string(counts[i]) +
+                                            " neighbours, more than the row length " + std::to_string(stride));
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  const size_t N = natoms, NS = N * stride;
+  cudaStream_t s = h->stream;
+  if (natoms > 0) {
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_itypes, itypes, N * sizeof(int), cudaMemcpyHostToDevice, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_rijs, rijs, 3 * NS * sizeof(double), cudaMemcpyHostToDevice, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_js, js, NS * sizeof(int), cudaMemcpyHostToDevice, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_jtypes, jtypes, NS * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (counts) MTP_CUDA(h, cudaMemcpyAsync(h->d_counts, counts, N * sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  int st = run_device(h, natoms, stride, h->d_itypes, h->d_rijs, h->d_js, h->d_jtypes, counts ? h->d_counts : nullptr,
+                      true, h->d_F, (flags & MTP_VATOM) ? h->d_vatom : nullptr);
+  if (st != MTP_OK) return st;
+  MTP_CUDA(h, launch_totals(natoms, h->d_E, h->d_wown, h->d_partials, h->d_tot, s));
+  if (natoms > 0) {
+    MTP_CUDA(h, cudaMemcpyAsync(forces, h->d_F, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (flags & MTP_EATOM) MTP_CUDA(h, cudaMemcpyAsync(eatom, h->d_E, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (flags & MTP_VATOM)
+      MTP_CUDA(h, cudaMemcpyAsync(vatom, h->d_vatom, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  MTP_CUDA(h, cudaMemcpyAsync(h->h_tot, h->d_tot, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  st = read_err_flags(h);   // synchronises the stream
+  if (st != MTP_OK) return st;
+  if (flags & MTP_EFLAG) *energy = h->h_tot[0];
+  if (flags & MTP_VFLAG)
+    for (int c = 0; c < 6; ++c) virial[c] = h->h_tot[1 + c];
+  h->calls++;
+  double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  h->total_ms += ms;
+  if (h->debug >= 2) std::fprintf(stderr, "[mtp_b200] call %lld: natoms=%d %.3f ms\n", h->calls, natoms, ms);
+  return MTP_OK;
+}
+
+int mtp_execute_potential(mtp_handle* h, int natoms, int nneigh_total, const double* const* atom_positions,
+                          const int* atom_types, const int* const* neighbor_lists, const int* neighbor_counts,
+                          const int* const* neighbor_types_lists, double volume, double* energy, double** forces,
+                          double* stress) {
+  (void)nneigh_total;
+  if (!h) return MTP_E_INVALID;
+  if (natoms < 0) return fail(h, MTP_E_INVALID, "natoms must be >= 0");
+  if (natoms > h->max_atoms) return fail(h, MTP_E_CAPACITY, "natoms exceeds max_atoms");
+  if (natoms > 0 && (!atom_positions || !atom_types || !neighbor_lists || !neighbor_counts || !neighbor_types_lists ||
+                     !forces || !energy || !stress))
+    return fail(h, MTP_E_INVALID, "null argument");
+  const int stride = h->max_nbr;
+  // pack the per-atom rows into the flat layout (what the reference bridge
+  // copies into its NumPy buffers, zero_overhead.cpp:94-116)
+  std::vector<double> rij(static_cast<size_t>(natoms) * stride * 3, 0.0);
+  std::vector<int> js(static_cast<size_t>(natoms) * stride, -1), jt(static_cast<size_t>(natoms) * stride, -1);
+  std::vector<int> cnt(natoms);
+  for (int i = 0; i < natoms; ++i) {
+    const int c = neighbor_counts[i];
+    if (c < 0 || c > stride)
+      return fail(h, MTP_E_CAPACITY, "atom " + std::to_string(i) + " has " + std::to_string(c) +
+                                          " neighbours, more than MAX_ATOMS_PER_NEIGHBOR");
+    cnt[i] = c;
+    if (c == 0) continue;
+    std::memcpy(&rij[static_cast<size_t>(i) * stride * 3], atom_positions[i], 3 * c * sizeof(double));
+    std::memcpy(&js[static_cast<size_t>(i) * stride], neighbor_lists[i], c * sizeof(int));
+    std::memcpy(&jt[static_cast<size_t>(i) * stride], neighbor_types_lists[i], c * sizeof(int));
+  }
+  std::vector<double> f(3 * static_cast<size_t>(natoms));
+  double vir[6] = {0, 0, 0, 0, 0, 0}, e = 0.0;
+  int st = mtp_compute(h, natoms, stride, atom_types, rij.data(), js.data(), jt.data(), cnt.data(),
+                       MTP_EFLAG | MTP_VFLAG, &e, f.data(), vir, nullptr, nullptr);
+  if (st != MTP_OK) return st;
+  *energy = e;
+  for (int i = 0; i < natoms; ++i)
+    for (int c = 0; c < 3; ++c) forces[i][c] = f[3 * static_cast<size_t>(i) + c];
+  // reference stress: +sym(sum r g)/V, order xx,yy,zz,yz,xz,xy (jax_backend.py:355-360)
+  const double iv = 1.0 / volume;
+  stress[0] = -vir[0] * iv;
+  stress[1] = -vir[1] * iv;
+  stress[2] = -vir[2] * iv;
+  stress[3] = -vir[5] * iv;
+  stress[4] = -vir[4] * iv;
+  stress[5] = -vir[3] * iv;
+  return MTP_OK;
+}
+
+int mtp_compute_batch_device(mtp_handle* h, int natoms, int stride, int nconfig, const int* d_itypes,
+                             const double* d_rijs, const int* d_js, const int* d_jtypes, const int* d_counts,
+                             const int* d_cfg, const double* d_volumes, double* d_energy, double* d_forces,
+                             double* d_stress) {
+  if (!h) return MTP_E_INVALID;
+  if (natoms < 0 || stride <= 0 || nconfig < 0) return fail(h, MTP_E_INVALID, "bad sizes");
+  if (natoms > h->max_atoms) return fail(h, MTP_E_CAPACITY, "natoms exceeds max_atoms");
+  if (stride > h->max_nbr) return fail(h, MTP_E_CAPACITY, "nbr_stride exceeds max_nbr");
+  if (natoms > 0 && (!d_itypes || !d_rijs || !d_js || !d_jtypes || !d_cfg || !d_volumes || !d_energy ||
+                     !d_forces || !d_stress))
+    return fail(h, MTP_E_INVALID, "null pointer");
+  if (nconfig + 1 > h->cfg_cap) {
+    if (h->d_cfg_ptr) cudaFree(h->d_cfg_ptr);
+    h->d_cfg_ptr = nullptr;
+    MTP_CUDA(h, dalloc(&h->d_cfg_ptr, nconfig + 1));
+    h->cfg_cap = nconfig + 1;
+  }
+  MTP_CUDA(h, launch_config_ptr(natoms, nconfig, d_cfg, h->d_cfg_ptr, h->d_err, h->stream));
+  int st = run_device(h, natoms, stride, d_itypes, d_rijs, d_js, d_jtypes, d_counts, true, d_forces, nullptr);
+  if (st != MTP_OK) return st;
+  MTP_CUDA(h, launch_config_totals(natoms, nconfig, h->d_cfg_ptr, h->d_E, h->d_wown, d_volumes, d_energy, d_stress,
+                                   h->stream));
+  h->calls++;
+  return MTP_OK;
+}
+
+int mtp_adjoint_batch_device(mtp_handle* h, int natoms, int stride, int nconfig, const int* d_itypes,
+                             const double* d_rijs, const int* d_js, const int* d_jtypes, const int* d_counts,
+                             const int* d_cfg, const double* d_volumes, const double* d_gE, const double* d_gF,
+                             const double* d_gS, double* d_gspecies, double* d_gmoment, double* d_gradial) {
+  if (!h) return MTP_E_INVALID;
+  if (natoms < 0 || stride <= 0 || nconfig < 0) return fail(h, MTP_E_INVALID, "bad sizes");
+  if (natoms > h->max_atoms) return fail(h, MTP_E_CAPACITY, "natoms exceeds max_atoms");
+  if (stride > h->max_nbr) return fail(h, MTP_E_CAPACITY, "nbr_stride exceeds max_nbr");
+  if (!d_gspecies || !d_gmoment || !d_gradial) return fail(h, MTP_E_INVALID, "null gradient pointer");
+  if (natoms > 0 && (!d_itypes || !d_rijs || !d_js || !d_jtypes || !d_cfg || !d_volumes || !d_gE || !d_gF || !d_gS))
+    return fail(h, MTP_E_INVALID, "null pointer");
+  DeviceSchedule* ds = nullptr;
+  int st = get_schedule(h, h->threads, &ds);
+  if (st != MTP_OK) return st;
+  DevModel md = make_model(h, *ds);
+  TrainIO tio{};
+  tio.natoms = natoms;
+  tio.nbr_stride = stride;
+  tio.nconfig = nconfig;
+  tio.itypes = d_itypes;
+  tio.rijs = d_rijs;
+  tio.js = d_js;
+  tio.jtypes = d_jtypes;
+  tio.counts = d_counts;
+  tio.cfg = d_cfg;
+  tio.volumes = d_volumes;
+  tio.gE = d_gE;
+  tio.gF = d_gF;
+  tio.gS = d_gS;
+  tio.err = h->d_err;
+  std::string err;
+  cudaError_t ce = launch_adjoint(md, tio, h->threads, h->sm_count, h->train, d_gspecies, d_gmoment, d_gradial,
+                                  h->stream, err);
+  if (!err.empty()) return fail(h, MTP_E_CAPACITY, err);
+  if (ce != cudaSuccess) return cuda_fail(h, ce, "adjoint");
+  h->calls++;
+  return MTP_OK;
+}
+
+int mtp_measure_fma_peak(double* fp64, double* fp32) {
+  if (!fp64 || !fp32) return MTP_E_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return MTP_E_NODEVICE;
+  }
+  return measure_fma_peak(fp64, fp32) == cudaSuccess ? MTP_OK : MTP_E_CUDA;
+}
+
+}  // extern "C"

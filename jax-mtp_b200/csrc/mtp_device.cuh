@@ -1,0 +1,424 @@
+// mtp_device.cuh - sm_100a kernels of the MTP evaluator.
+//
+// One persistent thread block evaluates one centre atom at a time (a
+// grid-stride loop over atoms):
+//
+//   N1  neighbour staging: slots of the atom's padded row are read with
+//       coalesced loads, tested (t_j >= 0, |r| < max_dist), compacted with a
+//       warp ballot, and each kept neighbour gets its unit vector, distance,
+//       radial functions f_mu(d), f'_mu(d) (Chebyshev basis times the smooth
+//       cutoff, jax_backend.py:83-95, 108-160) and the powers of its unit
+//       vector components, all in shared memory;
+//   N2  basic moments m[(mu, a, b, c)] = sum_j f_mu(d_j) u_x^a u_y^b u_z^c
+//       (conversion.py:66-81), one thread per distinct monomial;
+//   T   contraction tree (conversion.py:95-102) by the lane programs of the
+//       schedule, then E_i = xi[t_i] + theta . m[mapping] (jax_backend.py:101-106);
+//   R   reverse programs: dE_i/dm for every moment, gathered per source, so
+//       no two threads ever add into the same value;
+//   N3  per neighbour: dE_i/dr_ij from dE_i/dm of the basic moments
+//       (the analytic form of jax.value_and_grad at jax_backend.py:56),
+//       written to the per-slot gradient array.
+//
+// Forces then come from a per-atom gather (k_force_gather): the atom's own
+// slot gradients minus the gradients of the slots that point at it, in a
+// fixed order, so results are bitwise reproducible without atomics
+// (jax_backend.py:263-303 uses an atomic segment_sum instead).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mtp_model.hpp"
+
+namespace mtp {
+
+enum ErrBits : int { kErrNonFinite = 1, kErrSpecies = 2, kErrCapacity = 4 };
+
+struct DevPass {
+  int offset;
+  int steps;
+};
+
+// Everything the evaluation kernel needs about the potential (device pointers).
+struct DevModel {
+  const uint2* entries;
+  DevPass fwd[kMaxPasses];
+  DevPass rev[kMaxPasses];
+  int nfwd, nrev;
+  const double* radial;     // [S][S][R][K]
+  const double* species;    // [S]
+  const double* theta;      // [Sa]
+  const int* mapping;       // [Sa]
+  const int* seed_idx;      // [nseed]
+  const double* seed_val;   // [nseed]
+  const int* zero_list;     // [nzero]
+  const int* mono_abc;      // [P][4]
+  const int* mono_k;        // [P][kMaxR]
+  int nseed, nzero;
+  int S, R, K, M, B, P, D, Sa;
+  int v_m, v_dm, v_zero, v_one, v_size;
+  double scaling, rmin, rmax;
+};
+
+struct DevIO {
+  int natoms;
+  int nbr_stride;
+  int n_pad;                // staging rows (>= max count, <= nbr_stride rounded)
+  const int* itypes;        // [natoms]
+  const double* rijs;       // [natoms][nbr_stride][3]
+  const int* jtypes;        // [natoms][nbr_stride]
+  const int* counts;        // [natoms] or null
+  double* site_energy;      // [natoms]
+  double* pair_grad;        // [natoms][nbr_stride][3]
+  int* err;                 // error bits
+  void* vscratch;           // [grid][v_size] value space when it lives in global memory
+};
+
+// Shared-memory carve of the evaluation kernel.
+struct SmemLayout {
+  int pws;        // stride of a power row (3 (D+1), rounded up to odd)
+  size_t v, rad, u, f, fp, pw, slot, abc, mk, red, cnt, total;
+};
+
+template <typename T>
+__host__ __device__ inline SmemLayout smem_layout(int v_size, int S, int R, int K, int P, int D, int n_pad,
+                                                  int threads) {
+  SmemLayout L;
+  L.pws = 3 * (D + 1);
+  if ((L.pws & 1) == 0) L.pws += 1;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = (o + 15) & ~size_t(15);
+    o = at + bytes;
+    return at;
+  };
+  L.v = take(sizeof(T) * v_size);
+  L.rad = take(sizeof(T) * S * S * R * K);
+  L.u = take(sizeof(T) * 4 * n_pad);
+  L.f = take(sizeof(T) * R * n_pad);
+  L.fp = take(sizeof(T) * R * n_pad);
+  L.pw = take(sizeof(T) * L.pws * n_pad);
+  L.slot = take(sizeof(int) * n_pad);
+  L.abc = take(sizeof(int) * 4 * P);
+  L.mk = take(sizeof(int) * kMaxR * P);
+  L.red = take(sizeof(double) * (threads / 32));
+  L.cnt = take(sizeof(int) * (threads / 32 + 1));
+  L.total = (o + 15) & ~size_t(15);
+  return L;
+}
+
+__device__ __forceinline__ double dev_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float dev_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double dev_fma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float dev_fma(float a, float b, float c) { return fmaf(a, b, c); }
+
+// Execute one lane program pass: acc += c * V[a] * V[b]; flush on STORE/ADD.
+template <typename T>
+__device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int steps, int lanes, int tid,
+                                         T* __restrict__ V) {
+  const uint2* p = ent + tid;
+  T acc = T(0);
+#pragma unroll 4
+  for (int s = 0; s < steps; ++s) {
+    uint2 e = __ldg(p + static_cast<size_t>(s) * lanes);
+    const T c = static_cast<T>(e.y >> 18);
+    acc = dev_fma(c * V[e.x & 0xFFFFu], V[e.x >> 16], acc);
+    const uint32_t op = (e.y >> 16) & 3u;
+    if (op) {
+      const uint32_t d = e.y & 0xFFFFu;
+      if (op == kOpStore) V[d] = acc;
+      else V[d] += acc;
+      acc = T(0);
+    }
+  }
+}
+
+// Deterministic block sum of one double per thread (valid in thread 0).
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < static_cast<int>(blockDim.x >> 5); ++i) s += red[i];
+  }
+  __syncthreads();
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// evaluation kernel
+// ---------------------------------------------------------------------------
+// kVGlobal: the per-atom value space (moments, adjoints, partials) is a
+// private slice of global memory (L1/L2-resident) instead of shared memory;
+// used when it does not fit in shared memory (level 28 in FP64).
+template <typename T, bool kVGlobal>
+__global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int NT = blockDim.x;
+  const int tid = threadIdx.x;
+  const SmemLayout L = smem_layout<T>(kVGlobal ? 0 : md.v_size, md.S, md.R, md.K, md.P, md.D, io.n_pad, NT);
+  T* V = kVGlobal ? reinterpret_cast<T*>(io.vscratch) + static_cast<size_t>(blockIdx.x) * md.v_size
+                  : reinterpret_cast<T*>(smem + L.v);
+  T* sRad = reinterpret_cast<T*>(smem + L.rad);
+  T* sU = reinterpret_cast<T*>(smem + L.u);
+  T* sF = reinterpret_cast<T*>(smem + L.f);
+  T* sFp = reinterpret_cast<T*>(smem + L.fp);
+  T* sPw = reinterpret_cast<T*>(smem + L.pw);
+  int* sSlot = reinterpret_cast<int*>(smem + L.slot);
+  int* sAbc = reinterpret_cast<int*>(smem + L.abc);
+  int* sMk = reinterpret_cast<int*>(smem + L.mk);
+  double* sRed = reinterpret_cast<double*>(smem + L.red);
+  int* sCnt = reinterpret_cast<int*>(smem + L.cnt);
+
+  const int S = md.S, R = md.R, K = md.K, P = md.P, D1 = md.D + 1, pws = L.pws;
+  // per-block constants
+  for (int x = tid; x < S * S * R * K; x += NT) sRad[x] = static_cast<T>(md.radial[x]);
+  for (int x = tid; x < 4 * P; x += NT) sAbc[x] = md.mono_abc[x];
+  for (int x = tid; x < kMaxR * P; x += NT) sMk[x] = md.mono_k[x];
+  for (int x = tid; x < md.nzero; x += NT) V[md.v_m + md.zero_list[x]] = T(0);
+  if (tid == 0) {
+    V[md.v_zero] = T(0);
+    V[md.v_one] = T(1);
+  }
+  const T rmin = static_cast<T>(md.rmin), rmax = static_cast<T>(md.rmax);
+  const T inv_range = static_cast<T>(1.0 / (md.rmax - md.rmin));
+  const T rsum = static_cast<T>(md.rmin + md.rmax);
+  const T scal = static_cast<T>(md.scaling);
+  __syncthreads();
+
+  for (int atom = blockIdx.x; atom < io.natoms; atom += gridDim.x) {
+    int it = __ldg(io.itypes + atom);
+    if (it < 0 || it >= S) {
+      if (tid == 0) atomicOr(io.err, kErrSpecies);
+      it = 0;
+    }
+    int cnt = io.counts ? __ldg(io.counts + atom) : io.nbr_stride;
+    if (cnt > io.n_pad || cnt < 0) {
+      if (tid == 0) atomicOr(io.err, kErrCapacity);
+      cnt = cnt < 0 ? 0 : io.n_pad;
+    }
+    const double* rrow = io.rijs + static_cast<size_t>(atom) * io.nbr_stride * 3;
+    const int* trow = io.jtypes + static_cast<size_t>(atom) * io.nbr_stride;
+    double* grow = io.pair_grad + static_cast<size_t>(atom) * io.nbr_stride * 3;
+
+    // ---- N1: stage the valid neighbours ---------------------------------
+    int nv = 0;
+    for (int s0 = 0; s0 < io.nbr_stride; s0 += NT) {
+      const int s = s0 + tid;
+      bool valid = false;
+      T rx = T(0), ry = T(0), rz = T(0), d = T(0);
+      int jt = -1;
+      if (s < io.nbr_stride) {
+        if (s < cnt) {
+          jt = __ldg(trow + s);
+          rx = static_cast<T>(__ldg(rrow + 3 * s));
+          ry = static_cast<T>(__ldg(rrow + 3 * s + 1));
+          rz = static_cast<T>(__ldg(rrow + 3 * s + 2));
+          if (jt >= S) {
+            atomicOr(io.err, kErrSpecies);
+            jt = -1;
+          }
+          const T r2 = rx * rx + ry * ry + rz * rz;
+          d = dev_sqrt(r2);
+          valid = (jt >= 0) && (r2 > T(0)) && (d < rmax);
+        }
+        if (!valid) {
+          grow[3 * s] = 0.0;
+          grow[3 * s + 1] = 0.0;
+          grow[3 * s + 2] = 0.0;
+        }
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, valid);
+      const int w = tid >> 5, l = tid & 31;
+      if (l == 0) sCnt[w] = __popc(bal);
+      __syncthreads();
+      if (tid == 0) {
+        int acc = 0;
+        for (int i = 0; i < (NT >> 5); ++i) {
+          int c = sCnt[i];
+          sCnt[i] = acc;
+          acc += c;
+        }
+        sCnt[NT >> 5] = acc;
+      }
+      __syncthreads();
+      if (valid) {
+        const int q = nv + sCnt[w] + __popc(bal & ((1u << l) - 1u));
+        const T inv_d = T(1) / d;
+        const T ux = rx * inv_d, uy = ry * inv_d, uz = rz * inv_d;
+        sU[4 * q] = ux;
+        sU[4 * q + 1] = uy;
+        sU[4 * q + 2] = uz;
+        sU[4 * q + 3] = d;
+        sSlot[q] = s;
+        // Chebyshev T_n(x) and dT_n/dx by their recurrences, folded into
+        // sum_n c[t_i, t_j, mu, n] T_n for every mu as the terms appear
+        const T x = (T(2) * d - rsum) * inv_range;
+        const T dxdd = T(2) * inv_range;
+        const T* c = sRad + (static_cast<size_t>(it) * S + jt) * R * K;
+        T base[kMaxR], dbase[kMaxR];
+#pragma unroll
+        for (int mu = 0; mu < kMaxR; ++mu) {
+          base[mu] = mu < R ? c[mu * K] : T(0);   // T_0 = 1, T_0' = 0
+          dbase[mu] = T(0);
+        }
+        T t_prev = T(1), t_cur = x, dt_prev = T(0), dt_cur = T(1);
+        for (int n = 1; n < K; ++n) {
+#pragma unroll
+          for (int mu = 0; mu < kMaxR; ++mu) {
+            if (mu < R) {
+              base[mu] = dev_fma(c[mu * K + n], t_cur, base[mu]);
+              dbase[mu] = dev_fma(c[mu * K + n], dt_cur, dbase[mu]);
+            }
+          }
+          const T t_next = T(2) * x * t_cur - t_prev;
+          const T dt_next = T(2) * t_cur + T(2) * x * dt_cur - dt_prev;
+          t_prev = t_cur;
+          t_cur = t_next;
+          dt_prev = dt_cur;
+          dt_cur = dt_next;
+        }
+        const T gap = rmax - d;
+        const T smooth = gap * gap;
+#pragma unroll
+        for (int mu = 0; mu < kMaxR; ++mu) {
+          if (mu < R) {
+            sF[q * R + mu] = scal * smooth * base[mu];
+            sFp[q * R + mu] = scal * (T(-2) * gap * base[mu] + smooth * dbase[mu] * dxdd);
+          }
+        }
+        T* pw = sPw + q * pws;
+        T px = T(1), py = T(1), pz = T(1);
+        for (int e = 0; e < D1; ++e) {
+          pw[e] = px;
+          pw[D1 + e] = py;
+          pw[2 * D1 + e] = pz;
+          px *= ux;
+          py *= uy;
+          pz *= uz;
+        }
+      }
+      nv += sCnt[NT >> 5];
+      __syncthreads();
+    }
+
+    // ---- N2: basic moments ----------------------------------------------
+    for (int p = tid; p < P; p += NT) {
+      const int a = sAbc[4 * p], b = sAbc[4 * p + 1], cc = sAbc[4 * p + 2];
+      T acc[kMaxR];
+#pragma unroll
+      for (int mu = 0; mu < kMaxR; ++mu) acc[mu] = T(0);
+      for (int q = 0; q < nv; ++q) {
+        const T* pw = sPw + q * pws;
+        const T mono = pw[a] * pw[D1 + b] * pw[2 * D1 + cc];
+        const T* f = sF + q * R;
+#pragma unroll
+        for (int mu = 0; mu < kMaxR; ++mu)
+          if (mu < R) acc[mu] = dev_fma(f[mu], mono, acc[mu]);
+      }
+#pragma unroll
+      for (int mu = 0; mu < kMaxR; ++mu) {
+        if (mu < R) {
+          const int k = sMk[kMaxR * p + mu];
+          if (k >= 0) V[md.v_m + k] = acc[mu];
+        }
+      }
+    }
+    // adjoint seeds
+    for (int x = tid; x < md.M; x += NT) V[md.v_dm + x] = T(0);
+    __syncthreads();
+    for (int x = tid; x < md.nseed; x += NT) V[md.v_dm + md.seed_idx[x]] = static_cast<T>(md.seed_val[x]);
+
+    // ---- T: forward contraction passes ----------------------------------
+    for (int ps = 0; ps < md.nfwd; ++ps) {
+      run_pass<T>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, V);
+      __syncthreads();
+    }
+    // energy: E_i = xi[t_i] + sum_alpha theta_alpha m[map_alpha] in FP64
+    double epart = 0.0;
+    for (int a = tid; a < md.Sa; a += NT)
+      epart = fma(__ldg(md.theta + a), static_cast<double>(V[md.v_m + __ldg(md.mapping + a)]), epart);
+    const double esum = block_sum(epart, sRed);
+    if (tid == 0) {
+      const double e = __ldg(md.species + it) + esum;
+      io.site_energy[atom] = e;
+      if (!isfinite(e)) atomicOr(io.err, kErrNonFinite);
+    }
+
+    // ---- R: reverse passes (dE/dm) ---------------------------------------
+    for (int ps = 0; ps < md.nrev; ++ps) {
+      run_pass<T>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, V);
+      __syncthreads();
+    }
+
+    // ---- N3: dE_i/dr_ij per kept neighbour -------------------------------
+    {
+      int tpn = 32;
+      while (tpn > 1 && tpn * nv > NT) tpn >>= 1;
+      const int total = nv * tpn;
+      for (int base = 0; base < total; base += NT) {
+        const int idx = base + tid;
+        const bool active = idx < total;
+        const int q = active ? idx / tpn : 0;
+        const int sl = idx & (tpn - 1);
+        T Ssum = T(0), Gx = T(0), Gy = T(0), Gz = T(0);
+        if (active) {
+          T f[kMaxR], fp[kMaxR];
+#pragma unroll
+          for (int mu = 0; mu < kMaxR; ++mu) {
+            f[mu] = mu < R ? sF[q * R + mu] : T(0);
+            fp[mu] = mu < R ? sFp[q * R + mu] : T(0);
+          }
+          const T* pw = sPw + q * pws;
+          for (int p = sl; p < P; p += tpn) {
+            const int a = sAbc[4 * p], b = sAbc[4 * p + 1], cc = sAbc[4 * p + 2];
+            T W = T(0), Wp = T(0);
+#pragma unroll
+            for (int mu = 0; mu < kMaxR; ++mu) {
+              if (mu < R) {
+                const int k = sMk[kMaxR * p + mu];
+                if (k >= 0) {
+                  const T g = V[md.v_dm + k];
+                  W = dev_fma(g, f[mu], W);
+                  Wp = dev_fma(g, fp[mu], Wp);
+                }
+              }
+            }
+            const T px = pw[a], py = pw[D1 + b], pz = pw[2 * D1 + cc];
+            Ssum = dev_fma(Wp, px * py * pz, Ssum);
+            const T am = static_cast<T>(a), bm = static_cast<T>(b), cm = static_cast<T>(cc);
+            Gx = dev_fma(W * am, pw[a > 0 ? a - 1 : 0] * py * pz, Gx);
+            Gy = dev_fma(W * bm, px * pw[D1 + (b > 0 ? b - 1 : 0)] * pz, Gy);
+            Gz = dev_fma(W * cm, px * py * pw[2 * D1 + (cc > 0 ? cc - 1 : 0)], Gz);
+          }
+        }
+        for (int o = tpn >> 1; o > 0; o >>= 1) {
+          Ssum += __shfl_xor_sync(0xffffffffu, Ssum, o);
+          Gx += __shfl_xor_sync(0xffffffffu, Gx, o);
+          Gy += __shfl_xor_sync(0xffffffffu, Gy, o);
+          Gz += __shfl_xor_sync(0xffffffffu, Gz, o);
+        }
+        if (active && sl == 0) {
+          const T ux = sU[4 * q], uy = sU[4 * q + 1], uz = sU[4 * q + 2], d = sU[4 * q + 3];
+          const T ug = ux * Gx + uy * Gy + uz * Gz;
+          const T inv_d = T(1) / d;
+          const T gx = ux * Ssum + (Gx - ux * ug) * inv_d;
+          const T gy = uy * Ssum + (Gy - uy * ug) * inv_d;
+          const T gz = uz * Ssum + (Gz - uz * ug) * inv_d;
+          const int s = sSlot[q];
+          grow[3 * s] = static_cast<double>(gx);
+          grow[3 * s + 1] = static_cast<double>(gy);
+          grow[3 * s + 2] = static_cast<double>(gz);
+          if (!(isfinite(static_cast<double>(gx)) && isfinite(static_cast<double>(gy)) &&
+                isfinite(static_cast<double>(gz))))
+            atomicOr(io.err, kErrNonFinite);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace mtp

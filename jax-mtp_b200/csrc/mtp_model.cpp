@@ -1,0 +1,557 @@
+// mtp_model.cpp - .mtp parsing and contraction-schedule construction (host).
+#include "mtp_model.hpp"
+
+#include <algorithm>
+#include <cctype>
+#include <climits>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <map>
+#include <numeric>
+#include <queue>
+#include <sstream>
+
+namespace mtp {
+
+// ---------------------------------------------------------------------------
+// .mtp parsing (format of motep_original_files/mtp.py:31-70)
+// ---------------------------------------------------------------------------
+namespace {
+
+std::string trim(const std::string& s) {
+  size_t a = 0, b = s.size();
+  while (a < b && std::isspace(static_cast<unsigned char>(s[a]))) ++a;
+  while (b > a && std::isspace(static_cast<unsigned char>(s[b - 1]))) --b;
+  return s.substr(a, b - a);
+}
+
+bool parse_int(const std::string& s, int& v) {
+  std::string t = trim(s);
+  if (t.empty()) return false;
+  char* end = nullptr;
+  long x = std::strtol(t.c_str(), &end, 10);
+  if (*end != '\0' || x < INT_MIN || x > INT_MAX) return false;
+  v = static_cast<int>(x);
+  return true;
+}
+
+bool parse_double(const std::string& s, double& v) {
+  std::string t = trim(s);
+  if (t.empty()) return false;
+  char* end = nullptr;
+  v = std::strtod(t.c_str(), &end);
+  return *end == '\0';
+}
+
+// "{a, b, c}" -> numbers
+template <typename T>
+bool parse_list(const std::string& s, std::vector<T>& out) {
+  std::string t = trim(s);
+  if (t.size() < 2 || t.front() != '{' || t.back() != '}') return false;
+  out.clear();
+  const char* p = t.c_str() + 1;
+  const char* e = t.c_str() + t.size() - 1;
+  while (p < e) {
+    while (p < e && (std::isspace(static_cast<unsigned char>(*p)) || *p == ',')) ++p;
+    if (p >= e) break;
+    char* end = nullptr;
+    double x = std::strtod(p, &end);
+    if (end == p) return false;
+    out.push_back(static_cast<T>(x));
+    if (std::is_integral<T>::value && x != std::floor(x)) return false;
+    p = end;
+  }
+  return true;
+}
+
+// "{{a,b,c,d}, {...}}" -> flat ints, 4 per row
+bool parse_table(const std::string& s, std::vector<int>& out) {
+  std::string t = trim(s);
+  if (t.size() < 2 || t.front() != '{' || t.back() != '}') return false;
+  out.clear();
+  const char* p = t.c_str() + 1;
+  const char* e = t.c_str() + t.size() - 1;
+  while (p < e) {
+    while (p < e && *p != '{') {
+      if (!std::isspace(static_cast<unsigned char>(*p)) && *p != ',') return false;
+      ++p;
+    }
+    if (p >= e) break;
+    ++p;  // '{'
+    int n = 0;
+    while (p < e && *p != '}') {
+      while (p < e && (std::isspace(static_cast<unsigned char>(*p)) || *p == ',')) ++p;
+      if (*p == '}') break;
+      char* end = nullptr;
+      long x = std::strtol(p, &end, 10);
+      if (end == p) return false;
+      out.push_back(static_cast<int>(x));
+      ++n;
+      p = end;
+    }
+    if (p >= e || *p != '}' || n != 4) return false;
+    ++p;
+  }
+  return true;
+}
+
+}  // namespace
+
+bool parse_mtp_text(const std::string& text, Potential& pot, std::string& err) {
+  pot = Potential();
+  std::vector<std::string> lines;
+  {
+    std::istringstream is(text);
+    std::string l;
+    while (std::getline(is, l)) lines.push_back(l);
+  }
+  bool header = false, have_radial = false;
+  bool have_basic = false, have_times = false, have_map = false, have_sp = false, have_mc = false;
+  int basic_count = -1, times_count = -1;
+  for (size_t i = 0; i < lines.size(); ++i) {
+    std::string line = trim(lines[i]);
+    if (line.empty()) continue;
+    if (line == "MTP") { header = true; continue; }
+    if (line == "radial_coeffs") {
+      if (pot.S <= 0 || pot.R <= 0 || pot.K <= 0) {
+        err = "radial_coeffs block before species_count/radial_funcs_count/radial_basis_size";
+        return false;
+      }
+      pot.radial.assign(static_cast<size_t>(pot.S) * pot.S * pot.R * pot.K, NAN);
+      std::vector<char> seen(static_cast<size_t>(pot.S) * pot.S, 0);
+      for (int pair = 0; pair < pot.S * pot.S; ++pair) {
+        if (++i >= lines.size()) { err = "truncated radial_coeffs block"; return false; }
+        std::string hdr = trim(lines[i]);
+        size_t dash = hdr.find('-');
+        int a = -1, b = -1;
+        if (dash == std::string::npos || !parse_int(hdr.substr(0, dash), a) ||
+            !parse_int(hdr.substr(dash + 1), b) || a < 0 || b < 0 || a >= pot.S || b >= pot.S) {
+          err = "bad species pair line '" + hdr + "' in radial_coeffs";
+          return false;
+        }
+        seen[a * pot.S + b] = 1;
+        for (int mu = 0; mu < pot.R; ++mu) {
+          if (++i >= lines.size()) { err = "truncated radial_coeffs block"; return false; }
+          std::vector<double> row;
+          if (!parse_list(lines[i], row) || static_cast<int>(row.size()) != pot.K) {
+            err = "radial_coeffs row must hold radial_basis_size numbers";
+            return false;
+          }
+          std::copy(row.begin(), row.end(),
+                    pot.radial.begin() + ((static_cast<size_t>(a) * pot.S + b) * pot.R + mu) * pot.K);
+        }
+      }
+      for (char c : seen)
+        if (!c) { err = "radial_coeffs does not cover every species pair"; return false; }
+      have_radial = true;
+      continue;
+    }
+    size_t eq = line.find('=');
+    if (eq == std::string::npos) { err = "unrecognised line '" + line.substr(0, 60) + "'"; return false; }
+    std::string key = trim(line.substr(0, eq));
+    std::string val = trim(line.substr(eq + 1));
+    bool ok = true;
+    if (key == "version") pot.version = val;
+    else if (key == "potential_name") pot.potential_name = val;
+    else if (key == "potential_tag") pot.potential_tag = val;
+    else if (key == "radial_basis_type") pot.radial_basis_type = val;
+    else if (key == "scaling") ok = parse_double(val, pot.scaling);
+    else if (key == "min_dist") ok = parse_double(val, pot.min_dist);
+    else if (key == "max_dist") ok = parse_double(val, pot.max_dist);
+    else if (key == "species_count") ok = parse_int(val, pot.S);
+    else if (key == "radial_basis_size") ok = parse_int(val, pot.K);
+    else if (key == "radial_funcs_count") ok = parse_int(val, pot.R);
+    else if (key == "alpha_moments_count") ok = parse_int(val, pot.M);
+    else if (key == "alpha_index_basic_count") ok = parse_int(val, basic_count);
+    else if (key == "alpha_index_times_count") ok = parse_int(val, times_count);
+    else if (key == "alpha_scalar_moments") ok = parse_int(val, pot.Sa);
+    else if (key == "alpha_index_basic") { ok = parse_table(val, pot.basic); have_basic = ok; }
+    else if (key == "alpha_index_times") { ok = parse_table(val, pot.times); have_times = ok; }
+    else if (key == "alpha_moment_mapping") { ok = parse_list(val, pot.mapping); have_map = ok; }
+    else if (key == "species_coeffs") { ok = parse_list(val, pot.species); have_sp = ok; }
+    else if (key == "moment_coeffs") { ok = parse_list(val, pot.moment); have_mc = ok; }
+    // unknown keys are ignored, as the reference stores them as strings
+    if (!ok) { err = "bad value for '" + key + "'"; return false; }
+  }
+  if (!header) { err = "missing 'MTP' header line"; return false; }
+  if (pot.radial_basis_type != "RBChebyshev") {
+    err = "radial_basis_type '" + pot.radial_basis_type + "' is not RBChebyshev";
+    return false;
+  }
+  if (!have_radial) { err = "missing radial_coeffs (an untrained template has no coefficients)"; return false; }
+  if (!have_basic || !have_times || !have_map || !have_sp || !have_mc) {
+    err = "missing one of alpha_index_basic, alpha_index_times, alpha_moment_mapping, species_coeffs, moment_coeffs";
+    return false;
+  }
+  pot.B = static_cast<int>(pot.basic.size() / 4);
+  pot.T = static_cast<int>(pot.times.size() / 4);
+  if (basic_count >= 0 && basic_count != pot.B) { err = "alpha_index_basic_count does not match the table"; return false; }
+  if (times_count >= 0 && times_count != pot.T) { err = "alpha_index_times_count does not match the table"; return false; }
+  if (static_cast<int>(pot.mapping.size()) != pot.Sa) { err = "alpha_scalar_moments does not match alpha_moment_mapping"; return false; }
+  if (static_cast<int>(pot.moment.size()) != pot.Sa) { err = "moment_coeffs must have alpha_scalar_moments entries"; return false; }
+  if (static_cast<int>(pot.species.size()) != pot.S) { err = "species_coeffs must have species_count entries"; return false; }
+  if (pot.S <= 0 || pot.R <= 0 || pot.K <= 0 || pot.M <= 0) { err = "non-positive basis sizes"; return false; }
+  if (pot.R > kMaxR) { err = "radial_funcs_count above the supported 8"; return false; }
+  if (pot.K > kMaxK) { err = "radial_basis_size above the supported 16"; return false; }
+  if (!(pot.max_dist > pot.min_dist) || !(pot.max_dist > 0.0)) { err = "need max_dist > min_dist and max_dist > 0"; return false; }
+  if (pot.B > pot.M) { err = "more basic moments than moments"; return false; }
+  for (int k = 0; k < pot.B; ++k) {
+    const int* r = &pot.basic[4 * k];
+    if (r[0] < 0 || r[0] >= pot.R || r[1] < 0 || r[2] < 0 || r[3] < 0) {
+      err = "alpha_index_basic row out of range"; return false;
+    }
+    if (r[1] + r[2] + r[3] > kMaxDegree) { err = "monomial degree above the supported 12"; return false; }
+  }
+  for (int e = 0; e < pot.T; ++e) {
+    const int* r = &pot.times[4 * e];
+    if (r[0] < 0 || r[0] >= pot.M || r[1] < 0 || r[1] >= pot.M || r[3] < 0 || r[3] >= pot.M) {
+      err = "alpha_index_times refers to a moment out of range"; return false;
+    }
+  }
+  for (int v : pot.mapping)
+    if (v < 0 || v >= pot.M) { err = "alpha_moment_mapping refers to a moment out of range"; return false; }
+  for (double v : pot.radial)
+    if (!std::isfinite(v)) { err = "non-finite radial coefficient"; return false; }
+  return true;
+}
+
+bool parse_mtp_file(const std::string& path, Potential& pot, std::string& err) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) { err = "cannot open '" + path + "'"; return false; }
+  std::stringstream ss;
+  ss << f.rdbuf();
+  return parse_mtp_text(ss.str(), pot, err);
+}
+
+// ---------------------------------------------------------------------------
+// schedule
+// ---------------------------------------------------------------------------
+namespace {
+
+// Symbolic value-space operands resolved after the partial count is known.
+constexpr uint32_t kSymZero = 0x80000000u;
+constexpr uint32_t kSymOne = 0x80000001u;
+constexpr uint32_t kSymPartBase = 0xC0000000u;
+
+struct Side {
+  uint32_t a, b;
+  uint32_t c;
+};
+struct Job {
+  uint32_t dst;
+  uint32_t op;
+  std::vector<Side> sides;
+};
+struct RawEntry {
+  uint32_t a, b, dst, op, c;
+};
+struct RawPass {
+  int steps = 0;
+  std::vector<RawEntry> e;  // [steps][lanes]
+};
+
+// Lay jobs onto lanes (longest first onto the least loaded lane).
+RawPass lay_out(const std::vector<Job>& jobs, int lanes) {
+  std::vector<int> order(jobs.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return jobs[x].sides.size() > jobs[y].sides.size(); });
+  using LaneLoad = std::pair<size_t, int>;
+  std::priority_queue<LaneLoad, std::vector<LaneLoad>, std::greater<LaneLoad>> heap;
+  for (int l = 0; l < lanes; ++l) heap.push({0, l});
+  std::vector<std::vector<int>> lane_jobs(lanes);
+  for (int j : order) {
+    auto top = heap.top();
+    heap.pop();
+    lane_jobs[top.second].push_back(j);
+    heap.push({top.first + jobs[j].sides.size(), top.second});
+  }
+  RawPass p;
+  size_t steps = 0;
+  for (int l = 0; l < lanes; ++l) {
+    size_t n = 0;
+    for (int j : lane_jobs[l]) n += jobs[j].sides.size();
+    steps = std::max(steps, n);
+  }
+  p.steps = static_cast<int>(steps);
+  p.e.assign(steps * lanes, RawEntry{kSymZero, kSymZero, kSymZero, kOpNone, 0});
+  for (int l = 0; l < lanes; ++l) {
+    size_t s = 0;
+    for (int j : lane_jobs[l]) {
+      const Job& jb = jobs[j];
+      for (size_t k = 0; k < jb.sides.size(); ++k, ++s) {
+        RawEntry& r = p.e[s * lanes + l];
+        r.a = jb.sides[k].a;
+        r.b = jb.sides[k].b;
+        r.c = jb.sides[k].c;
+        r.dst = kSymZero;
+        r.op = kOpNone;
+        if (k + 1 == jb.sides.size()) {
+          r.dst = jb.dst;
+          r.op = jb.op;
+        }
+      }
+    }
+  }
+  return p;
+}
+
+// Split long jobs into chunks writing partial slots; returns the main pass and,
+// when anything was split, the combine pass.  `parts_used` gets the number of
+// partial slots the pass pair needs.
+void emit_jobs(const std::vector<Job>& jobs, int lanes, std::vector<RawPass>& out, int& parts_used) {
+  size_t total = 0;
+  for (const Job& j : jobs) total += j.sides.size();
+  if (total == 0) return;
+  size_t cap = std::max<size_t>(4, (total + lanes - 1) / lanes);
+  std::vector<Job> main_jobs, comb_jobs;
+  int parts = 0;
+  for (const Job& j : jobs) {
+    if (j.sides.empty()) continue;
+    if (j.sides.size() <= cap) {
+      main_jobs.push_back(j);
+      continue;
+    }
+    size_t nch = (j.sides.size() + cap - 1) / cap;
+    size_t per = (j.sides.size() + nch - 1) / nch;
+    Job comb{j.dst, j.op, {}};
+    for (size_t c0 = 0; c0 < j.sides.size(); c0 += per) {
+      Job ch{kSymPartBase + static_cast<uint32_t>(parts), kOpStore, {}};
+      ch.sides.assign(j.sides.begin() + c0, j.sides.begin() + std::min(j.sides.size(), c0 + per));
+      main_jobs.push_back(std::move(ch));
+      comb.sides.push_back(Side{kSymPartBase + static_cast<uint32_t>(parts), kSymOne, 1});
+      ++parts;
+    }
+    comb_jobs.push_back(std::move(comb));
+  }
+  out.push_back(lay_out(main_jobs, lanes));
+  if (!comb_jobs.empty()) out.push_back(lay_out(comb_jobs, lanes));
+  parts_used = std::max(parts_used, parts);
+}
+
+}  // namespace
+
+void seed_list(const Potential& pot, std::vector<int>& idx, std::vector<double>& val) {
+  std::map<int, double> acc;
+  for (int a = 0; a < pot.Sa; ++a) acc[pot.mapping[a]] += pot.moment[a];
+  idx.clear();
+  val.clear();
+  for (auto& kv : acc) {
+    idx.push_back(kv.first);
+    val.push_back(kv.second);
+  }
+}
+
+bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& err) {
+  s = Schedule();
+  s.lanes = lanes;
+  const int M = pot.M, B = pot.B, T = pot.T;
+  if (lanes <= 0 || lanes % 32 != 0) { err = "lanes must be a positive multiple of 32"; return false; }
+
+  // depth of every moment and the write-before-read property
+  std::vector<int> depth(M, 0), last_write(M, -1), first_read(M, INT_MAX), is_target(M, 0);
+  for (int e = 0; e < T; ++e) {
+    const int* r = &pot.times[4 * e];
+    if (r[2] < 0 || r[2] >= (1 << 14)) { err = "alpha_index_times multiplicity outside [0, 16383]"; return false; }
+    depth[r[3]] = std::max(depth[r[3]], std::max(depth[r[0]], depth[r[1]]) + 1);
+    last_write[r[3]] = e;
+    is_target[r[3]] = 1;
+    first_read[r[0]] = std::min(first_read[r[0]], e);
+    first_read[r[1]] = std::min(first_read[r[1]], e);
+  }
+  for (int k = 0; k < M; ++k) {
+    if (last_write[k] >= 0 && first_read[k] <= last_write[k]) {
+      err = "alpha_index_times reads a moment before its last contribution; unsupported order";
+      return false;
+    }
+  }
+  int maxd = 0;
+  for (int k = 0; k < M; ++k) maxd = std::max(maxd, depth[k]);
+  s.max_depth = maxd;
+
+  // value-space layout (partials resolved at the end)
+  s.v_m = 0;
+  s.v_dm = M;
+  s.v_part = 2 * M;
+
+  // monomials
+  std::map<std::tuple<int, int, int>, int> mono_of;
+  std::vector<std::tuple<int, int, int>> monos;
+  for (int k = 0; k < B; ++k) {
+    auto key = std::make_tuple(pot.basic[4 * k + 1], pot.basic[4 * k + 2], pot.basic[4 * k + 3]);
+    if (!mono_of.count(key)) {
+      mono_of[key] = static_cast<int>(monos.size());
+      monos.push_back(key);
+    }
+  }
+  s.P = static_cast<int>(monos.size());
+  s.mono_abc.assign(4 * s.P, 0);
+  s.mono_k.assign(kMaxR * s.P, -1);
+  s.D = 0;
+  for (int p = 0; p < s.P; ++p) {
+    int a, b, c;
+    std::tie(a, b, c) = monos[p];
+    s.mono_abc[4 * p] = a;
+    s.mono_abc[4 * p + 1] = b;
+    s.mono_abc[4 * p + 2] = c;
+    s.mono_abc[4 * p + 3] = a + b + c;
+    s.D = std::max(s.D, a + b + c);
+  }
+  for (int k = 0; k < B; ++k) {
+    int mu = pot.basic[4 * k];
+    int p = mono_of[std::make_tuple(pot.basic[4 * k + 1], pot.basic[4 * k + 2], pot.basic[4 * k + 3])];
+    if (s.mono_k[kMaxR * p + mu] >= 0) { err = "duplicate row in alpha_index_basic"; return false; }
+    s.mono_k[kMaxR * p + mu] = k;
+  }
+  // moments that are read but never written stay zero for the whole run
+  std::vector<char> read(M, 0);
+  for (int e = 0; e < T; ++e) { read[pot.times[4 * e]] = 1; read[pot.times[4 * e + 1]] = 1; }
+  for (int v : pot.mapping) read[v] = 1;
+  for (int k = B; k < M; ++k)
+    if (!is_target[k] && read[k]) s.zero_list.push_back(k);
+
+  std::vector<RawPass> fwd, rev;
+  int parts = 0;
+  // forward: one pass per target depth, jobs = targets in first-appearance order
+  for (int L = 1; L <= maxd; ++L) {
+    std::vector<Job> jobs;
+    std::map<int, int> job_of;
+    for (int e = 0; e < T; ++e) {
+      const int* r = &pot.times[4 * e];
+      if (depth[r[3]] != L) continue;
+      auto it = job_of.find(r[3]);
+      if (it == job_of.end()) {
+        job_of[r[3]] = static_cast<int>(jobs.size());
+        jobs.push_back(Job{static_cast<uint32_t>(s.v_m + r[3]), r[3] < B ? kOpAdd : kOpStore, {}});
+        it = job_of.find(r[3]);
+      }
+      jobs[it->second].sides.push_back(
+          Side{static_cast<uint32_t>(s.v_m + r[0]), static_cast<uint32_t>(s.v_m + r[1]), static_cast<uint32_t>(r[2])});
+    }
+    emit_jobs(jobs, lanes, fwd, parts);
+  }
+  // reverse: passes for target depth maxd..1 gather sides whose source has
+  // depth >= 1; every side into a depth-0 source waits for one final pass.
+  auto add_side = [&](std::vector<Job>& jobs, std::map<int, int>& job_of, int src, int tgt, int other, int mult) {
+    auto it = job_of.find(src);
+    if (it == job_of.end()) {
+      job_of[src] = static_cast<int>(jobs.size());
+      jobs.push_back(Job{static_cast<uint32_t>(s.v_dm + src), kOpAdd, {}});
+      it = job_of.find(src);
+    }
+    jobs[it->second].sides.push_back(
+        Side{static_cast<uint32_t>(s.v_dm + tgt), static_cast<uint32_t>(s.v_m + other), static_cast<uint32_t>(mult)});
+  };
+  for (int L = maxd; L >= 1; --L) {
+    std::vector<Job> jobs;
+    std::map<int, int> job_of;
+    for (int e = 0; e < T; ++e) {
+      const int* r = &pot.times[4 * e];
+      if (depth[r[3]] != L) continue;
+      if (depth[r[0]] >= 1) add_side(jobs, job_of, r[0], r[3], r[1], r[2]);
+      if (depth[r[1]] >= 1) add_side(jobs, job_of, r[1], r[3], r[0], r[2]);
+    }
+    emit_jobs(jobs, lanes, rev, parts);
+  }
+  {
+    std::vector<Job> jobs;
+    std::map<int, int> job_of;
+    for (int L = maxd; L >= 1; --L) {
+      for (int e = 0; e < T; ++e) {
+        const int* r = &pot.times[4 * e];
+        if (depth[r[3]] != L) continue;
+        if (depth[r[0]] == 0) add_side(jobs, job_of, r[0], r[3], r[1], r[2]);
+        if (depth[r[1]] == 0) add_side(jobs, job_of, r[1], r[3], r[0], r[2]);
+      }
+    }
+    emit_jobs(jobs, lanes, rev, parts);
+  }
+  s.n_part = parts;
+  s.v_zero = s.v_part + parts;
+  s.v_one = s.v_zero + 1;
+  s.v_size = s.v_one + 1;
+  if (s.v_size > 65535) { err = "value space above 65535 entries; basis too large"; return false; }
+  if (static_cast<int>(fwd.size() + rev.size()) > kMaxPasses * 2) { err = "too many passes"; return false; }
+
+  auto resolve = [&](uint32_t v) -> uint32_t {
+    if (v == kSymZero) return static_cast<uint32_t>(s.v_zero);
+    if (v == kSymOne) return static_cast<uint32_t>(s.v_one);
+    if (v >= kSymPartBase) return static_cast<uint32_t>(s.v_part) + (v - kSymPartBase);
+    return v;
+  };
+  auto flush_passes = [&](std::vector<RawPass>& raw, std::vector<Pass>& dst) {
+    for (RawPass& rp : raw) {
+      Pass p;
+      p.offset = static_cast<int>(s.entries.size() / 2);
+      p.steps = rp.steps;
+      for (const RawEntry& r : rp.e) {
+        uint32_t a = resolve(r.a), b = resolve(r.b), d = resolve(r.dst);
+        s.entries.push_back(a | (b << 16));
+        s.entries.push_back(d | (r.op << 16) | (r.c << 18));
+      }
+      dst.push_back(p);
+    }
+  };
+  flush_passes(fwd, s.fwd);
+  flush_passes(rev, s.rev);
+  // every operand and destination must lie inside the value space
+  for (size_t e = 0; e < s.entries.size(); e += 2) {
+    const uint32_t x = s.entries[e], y = s.entries[e + 1];
+    if ((x & 0xFFFFu) >= static_cast<uint32_t>(s.v_size) || (x >> 16) >= static_cast<uint32_t>(s.v_size) ||
+        (y & 0xFFFFu) >= static_cast<uint32_t>(s.v_size)) {
+      err = "internal error: schedule operand outside the value space";
+      return false;
+    }
+  }
+  if (static_cast<int>(s.fwd.size()) > kMaxPasses || static_cast<int>(s.rev.size()) > kMaxPasses) {
+    err = "too many passes";
+    return false;
+  }
+  return true;
+}
+
+double emulate_schedule(const Potential& pot, const Schedule& s, std::vector<double>& V) {
+  V.resize(s.v_size, 0.0);
+  for (int k : s.zero_list) V[s.v_m + k] = 0.0;
+  V[s.v_zero] = 0.0;
+  V[s.v_one] = 1.0;
+  auto run = [&](const Pass& p) {
+    // Lanes run one after another: the schedule guarantees that no lane reads
+    // a slot another lane writes in the same pass, so this equals the device.
+    std::vector<double> out;
+    std::vector<std::pair<int, std::pair<int, double>>> writes;
+    for (int l = 0; l < s.lanes; ++l) {
+      double acc = 0.0;
+      for (int st = 0; st < p.steps; ++st) {
+        size_t e = static_cast<size_t>(p.offset) + static_cast<size_t>(st) * s.lanes + l;
+        uint32_t x = s.entries[2 * e], y = s.entries[2 * e + 1];
+        int a = x & 0xFFFF, b = x >> 16, d = y & 0xFFFF, op = (y >> 16) & 3;
+        double c = static_cast<double>(y >> 18);
+        acc = std::fma(c * V[a], V[b], acc);
+        if (op != kOpNone) {
+          writes.push_back({d, {static_cast<int>(op), acc}});
+          acc = 0.0;
+        }
+      }
+    }
+    for (auto& w : writes) {
+      if (w.second.first == kOpStore) V[w.first] = w.second.second;
+      else V[w.first] += w.second.second;
+    }
+  };
+  for (const Pass& p : s.fwd) run(p);
+  double e = 0.0;
+  for (int a = 0; a < pot.Sa; ++a) e += pot.moment[a] * V[s.v_m + pot.mapping[a]];
+  for (int k = 0; k < pot.M; ++k) V[s.v_dm + k] = 0.0;
+  std::vector<int> si;
+  std::vector<double> sv;
+  seed_list(pot, si, sv);
+  for (size_t i = 0; i < si.size(); ++i) V[s.v_dm + si[i]] = sv[i];
+  for (const Pass& p : s.rev) run(p);
+  return e;
+}
+
+}  // namespace mtp

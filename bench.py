@@ -1,0 +1,434 @@
+#!/usr/bin/env python3
+"""Benchmark: MD atom-steps/s of the mixed-precision MTP kernel against the FP64
+kernel at a stated force error (the headline metric), on the mixed-vs-FP64
+workload at scale:
+
+    level-24 MTP (template tables, R=6, K=8), 3 species, cutoff 5.0 A,
+    fcc a = 3.6 A, 64^3 cells = 1,048,576 atoms, thermal displacement 0.08 A,
+    species uniform 1/3, NVE at 600 K, dt = 1 fs, device neighbour rebuild
+    every 10 steps (skin 0.3 A), each MD step captured as a CUDA graph.
+
+One "step" = one velocity-Verlet MD step (integration, r_ij packing, energy +
+forces + virial, and the neighbour rebuild at its cadence).  Inputs (1.6 GB of
+r_ij per step) are far larger than the 126 MB L2, so no flush is needed.
+
+Our arm (default) prints one JSON line with the mixed value, the FP64 value,
+the force/energy error of mixed vs FP64, the roofline of the evaluation
+kernel, the CPU baseline (C++/OpenMP FP64 restatement on the host cores) and
+the end-to-end number through the C ABI with host buffers.
+
+`--impl reference` times the reference algorithm's CPU implementation (the
+oracle port: JAX, which the reference needs, is not installed here) on the
+host cores for the same workload and metric.
+
+Multi-GPU: the path does not shard (one MD system per GPU); N ranks run N
+independent replicas ("scaling": "weak").
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "jax-mtp_b200"))
+sys.path.insert(0, ROOT)
+
+# level-24 tables, radial coefficients N(0, 0.1^2) from seed 5, moment coefficients
+# normalised per basis function to an RMS force of 0.5 eV/A (tests/golden/make_md_potentials.py)
+POT = os.path.join(ROOT, "tests", "golden", "potentials", "cfg2md_L24_S3.mtp")
+MASS = 55.845          # amu, one stated mass for every species
+REPS = 64
+STRIDE = 64
+SKIN = 0.3
+REBUILD = 10
+DT = 0.001
+TEMP = 600.0
+METRIC = "MD atom-steps/s, mixed vs FP64 kernel at stated force error; train cfg/s"
+
+
+def workload_config():
+    return {"workload": "MD NVE, level-24 MTP, 3 species, fcc a=3.6 A 64^3 = 1,048,576 atoms, 600 K, dt 1 fs, "
+                        "rebuild every 10 steps, CUDA-graph step",
+            "level": 24, "species": 3, "atoms": REPS ** 3 * 4, "nbr_stride": STRIDE, "cutoff": 5.0, "skin": SKIN,
+            "precision_headline": "mixed (FP32 radial/moments/tree, FP64 energy/virial/force accumulation)",
+            "l2_policy": "inputs (r_ij 1.6 GB/step) larger than L2; no flush",
+            "mass_amu": MASS, "parallelism": "replicas",
+            "potential": "cfg2md_L24_S3.mtp: radial N(0,0.1^2) seed 5, moment coefficients normalised per basis "
+                         "function to RMS force 0.5 eV/A (the N(0,0.01^2) draw gives 10^3 eV/A forces: no MD)"}
+
+
+def structure():
+    from mtp_b200 import synth
+    return synth.config2_structure(REPS)
+
+
+def algorithmic_flops(pot, counts_real: np.ndarray) -> float:
+    """Per launch: sum_i n_i (10 B + 6 R K + 6 K + 2 P + 75) + N (9 T + 2 Sa) (FMA = 2)."""
+    B = pot.alpha_index_basic_count
+    P = len({tuple(r) for r in pot.alpha_index_basic[:, 1:].tolist()})
+    R, K, T, Sa = pot.radial_funcs_count, pot.radial_basis_size, pot.alpha_index_times_count, pot.alpha_scalar_moments
+    per_nbr = 10 * B + 6 * R * K + 6 * K + 2 * P + 75
+    return float(counts_real.sum()) * per_nbr + len(counts_real) * (9 * T + 2 * Sa)
+
+
+def read_traffic():
+    """DRAM bytes per evaluation launch from the committed ncu summary, if any."""
+    f = os.path.join(ROOT, "profiles", "eval_kernel_l24_mixed.md")
+    if not os.path.exists(f):
+        return None
+    for line in open(f):
+        if line.startswith("traffic_bytes_per_launch_full_workload:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"mtp_clocks_{os.getpid()}_{gpu_index}.csv")
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+def cpu_baseline(pot, s, seconds: float = 12.0, sample_atoms: int = 2048):
+    """C++/OpenMP FP64 restatement on the host cores, bounded sample of the workload."""
+    from mtp_b200 import synth
+    from oracle.cpu_ref import CpuMTP
+    # a sample of centre atoms with their full neighbour rows
+    sub = synth.lattice_structure("fcc", 3.6, (8, 8, 8))       # 2048 atoms, same lattice / density
+    rng = np.random.default_rng(51)
+    sub.positions = sub.positions + rng.normal(0.0, 0.08, sub.positions.shape)
+    sub.types = np.random.default_rng(52).integers(0, 3, sub.natoms).astype(np.int32)
+    nd = synth.build_neighbors(sub, pot.max_dist, n_pad=STRIDE)
+    cpu = CpuMTP(pot)
+    cores = os.cpu_count() or 1
+    cpu.compute(nd.itypes, nd.rijs, nd.js, nd.jtypes, nd.counts, nthreads=cores)   # warm-up
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        cpu.compute(nd.itypes, nd.rijs, nd.js, nd.jtypes, nd.counts, nthreads=cores)
+        reps += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": nd.natoms * reps / dt, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+            "sample": f"{nd.natoms}-atom fcc a=3.6 cell of the same workload (energy+forces+virial, FP64), "
+                      f"{reps} evaluations in {dt:.1f} s"}
+
+
+# ----------------------------------------------------------------------------
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from mtp_b200.mtp_file import read_mtp
+    pot = read_mtp(POT)
+    steps, warm = args.steps, args.warmup
+    from mtp_b200 import synth
+    from oracle.cpu_ref import CpuMTP
+    sub = synth.lattice_structure("fcc", 3.6, (8, 8, 8))
+    rng = np.random.default_rng(51)
+    sub.positions = sub.positions + rng.normal(0.0, 0.08, sub.positions.shape)
+    sub.types = np.random.default_rng(52).integers(0, 3, sub.natoms).astype(np.int32)
+    nd = synth.build_neighbors(sub, pot.max_dist, n_pad=STRIDE)
+    cpu = CpuMTP(pot)
+    cores = os.cpu_count() or 1
+    for _ in range(warm):
+        cpu.compute(nd.itypes, nd.rijs, nd.js, nd.jtypes, nd.counts, nthreads=cores)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        cpu.compute(nd.itypes, nd.rijs, nd.js, nd.jtypes, nd.counts, nthreads=cores)
+    dt = time.perf_counter() - t0
+    value = nd.natoms * steps / dt
+    line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": warm, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": workload_config(),
+            "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+                             "sample": f"each step: energy+forces+virial of a {nd.natoms}-atom sample of the "
+                                       "workload (same lattice, density, species, potential) on the host cores; "
+                                       "the reference's JAX path cannot run (jax not installed)"},
+            "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------
+def time_md(md, steps: int, warmup: int, dist, device, sampler=None):
+    import torch
+    md.run(warmup, graphs=True)
+    torch.cuda.synchronize(device)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream(device)
+    if sampler is not None:
+        sampler.__enter__()
+    e0.record(stream)
+    md.run(steps, graphs=True)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    if sampler is not None:
+        sampler.__exit__()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t[0])
+        dist.barrier()
+    return ms
+
+
+def launches_per_step(rebuild: bool) -> int:
+    # verlet x2, pack, eval, gather, totals (partial + final)
+    n = 7
+    if rebuild:
+        # cell assign, scan (3), fill, sort, rows; incoming count, scan (3), fill, sort
+        n += 7 + 6
+    return n
+
+
+def run_ours(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+
+    from mtp_b200 import synth
+    from mtp_b200.engine import MTPEngine, measure_fma_peak
+    from mtp_b200.md import DeviceMD
+    from mtp_b200.mtp_file import read_mtp
+
+    pot = read_mtp(POT)
+    s = structure()
+    N = s.natoms
+    v0 = synth.maxwell_boltzmann(N, TEMP, MASS, seed=53 + rank)
+    masses = [MASS] * pot.species_count
+
+    results = {}
+    eng = {p: MTPEngine(POT, N, STRIDE, precision=p) for p in ("mixed", "fp64")}
+    mds = {}
+    for p in ("mixed", "fp64"):
+        mds[p] = DeviceMD(eng[p], s, masses, velocities=v0, dt=DT, skin=SKIN, rebuild_every=REBUILD, stride=STRIDE)
+    torch.cuda.synchronize(device)
+    # accuracy of mixed vs FP64 at the starting configuration (same neighbour rows)
+    fm, f64 = mds["mixed"].f.clone(), mds["fp64"].f.clone()
+    em, e64 = float(mds["mixed"].energy[0]), float(mds["fp64"].energy[0])
+    dF = (fm - f64).abs()
+    force_err = {"max_meV_per_A": float(dF.max()) * 1e3,
+                 "rms_meV_per_A": float(torch.sqrt(((fm - f64) ** 2).sum(1).mean())) * 1e3,
+                 "energy_meV_per_atom": abs(em - e64) / N * 1e3,
+                 "force_scale_eV_per_A": float(f64.abs().max())}
+    # real neighbours (d < max_dist) per atom, for the algorithmic FLOP count
+    rn = mds["fp64"].rijs.norm(dim=2)
+    valid = (mds["fp64"].jtypes >= 0) & (rn < pot.max_dist) & (rn > 0)
+    counts_real = valid.sum(1).cpu().numpy()
+    flops = algorithmic_flops(pot, counts_real)
+
+    for p in ("mixed", "fp64"):
+        mds[p].capture()
+    # timed regions
+    sampler = ClockSampler(local)
+    for p in ("fp64", "mixed"):
+        ms = time_md(mds[p], args.steps, args.warmup, dist, device, sampler if p == "mixed" else None)
+        eng[p].sync_status()
+        results[p] = {"ms": ms}
+    # the evaluation kernel alone: CUDA events around each launch (direct
+    # launches on the same rows; graph replays bypass the host-side hooks)
+    for p in ("fp64", "mixed"):
+        eng[p].set_stream(torch.cuda.current_stream(device).cuda_stream)
+        eng[p].profile(True)
+        for _ in range(max(3, min(args.steps, 10))):
+            mds[p]._forces(reuse=True)
+        kms, kn = eng[p].profile_read()
+        eng[p].profile(False)
+        results[p]["eval_ms_per_launch"] = kms / max(1, kn)
+        results[p]["eval_launches"] = kn
+    clocks = sampler.summary()
+    for p in ("mixed", "fp64"):
+        mds[p].release()
+    # drift over the timed run (energy per atom)
+    fp64_peak, fp32_peak = measure_fma_peak()
+
+    value = world * N * args.steps / (results["mixed"]["ms"] * 1e-3)
+    value64 = world * N * args.steps / (results["fp64"]["ms"] * 1e-3)
+    k_mixed = results["mixed"]["eval_ms_per_launch"] * 1e-3
+    k_64 = results["fp64"]["eval_ms_per_launch"] * 1e-3
+    achieved = flops / k_mixed / 1e12
+    achieved64 = flops / k_64 / 1e12
+    traffic = read_traffic()
+    nrebuild = sum(1 for k in range(args.warmup + 1, args.warmup + args.steps + 1) if k % REBUILD == 0)
+    launches = nrebuild * launches_per_step(True) + (args.steps - nrebuild) * launches_per_step(False)
+
+    # end to end through the C ABI with pinned host buffers (the pair-style boundary)
+    e2e = None
+    if rank == 0 and not args.skip_e2e:
+        e2e = run_e2e(eng["mixed"], mds["mixed"], N, args)
+
+    cpu = None
+    if rank == 0 and not args.skip_cpu:
+        cpu = cpu_baseline(pot, s, seconds=args.cpu_seconds)
+
+    for p in ("mixed", "fp64"):
+        eng[p].close()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": results["mixed"]["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (mixed; FP64 accumulation)", "data": "synthetic",
+            "config": workload_config(),
+            "fp64": {"value": value64, "unit": "atom-steps/s", "ms_per_step": results["fp64"]["ms"] / args.steps},
+            "mixed_over_fp64": value / value64,
+            "force_error_mixed_vs_fp64": force_err,
+            "roofline": {"bound": "fp32-fma", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
+                         "kernel": "k_mtp_eval<float> (mixed)", "flops_per_launch": flops,
+                         "kernel_ms": k_mixed * 1e3,
+                         "peak_source": "measured live: FP32 FMA-chain kernel (no FP32/FP64 CUDA-core peak in "
+                                        "MEASURED_PEAKS.json)",
+                         "fp64_kernel": {"achieved": achieved64, "peak": fp64_peak, "frac": achieved64 / fp64_peak
+                                         if fp64_peak else None, "kernel_ms": k_64 * 1e3}},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches * 1,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(eng, md, N, args):
+    """mtp_compute with pinned host buffers: H2D inputs + kernels + D2H results per step."""
+    import torch
+    stride = STRIDE
+    pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
+    it = pin((N,), torch.int32)
+    rij = pin((N, stride, 3), torch.float64)
+    js = pin((N, stride), torch.int32)
+    jt = pin((N, stride), torch.int32)
+    cnt = pin((N,), torch.int32)
+    F = pin((N, 3), torch.float64)
+    it[:] = md.types.cpu().numpy()
+    md._rebuild()
+    md.eng.pack_rij_device(md.x, md.cell, md.js, md.image, md.counts, md.rijs)
+    torch.cuda.synchronize()
+    rij[:] = md.rijs.cpu().numpy()
+    js[:] = md.js.cpu().numpy()
+    jt[:] = md.jtypes.cpu().numpy()
+    cnt[:] = md.counts.cpu().numpy()
+    from mtp_b200._lib import EFLAG, VFLAG, check, lib
+    import ctypes
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    e = np.zeros(1)
+    vir = np.zeros(6)
+    eng.use_own_stream()
+
+    def call():
+        code = lib().mtp_compute(eng.handle, N, stride, P(it), P(rij), P(js), P(jt), P(cnt), EFLAG | VFLAG, P(e), P(F),
+                                 P(vir), None, None)
+        check(code, eng.handle)
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        call()
+    steps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        call()
+    dt = time.perf_counter() - t0
+    h2d = N * 4 + N * stride * (24 + 4 + 4) + N * 4
+    d2h = N * 24 + 8 + 48
+    return {"value": N * steps / dt, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "steps": steps, "api": "mtp_compute (C ABI, pinned host buffers, synchronous)",
+            "note": "force call per MD step as the pair style makes it; integration not included"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

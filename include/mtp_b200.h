@@ -93,8 +93,11 @@ void mtp_destroy(mtp_handle* h);
 /* Text of the last error on this handle (or of the last failed mtp_create when h is NULL). */
 const char* mtp_last_error(const mtp_handle* h);
 
-/* Use this CUDA stream (a cudaStream_t) for all work of the handle; NULL = the handle's own. */
+/* Use this CUDA stream (a cudaStream_t) for all work of the handle; NULL is the
+ * legacy default stream (as in the CUDA runtime).  A new handle works on a
+ * non-blocking stream of its own; mtp_use_own_stream returns to it. */
 int mtp_set_stream(mtp_handle* h, void* cuda_stream);
+int mtp_use_own_stream(mtp_handle* h);
 
 /* Basis sizes of the loaded potential: out[0..7] = species_count, radial_funcs_count,
  * radial_basis_size, alpha_moments_count, alpha_index_basic_count,
@@ -201,6 +204,36 @@ int mtp_parse_info(const char* mtp_path, int* out8, char* err, int err_len);
  */
 int mtp_schedule_emulate(const char* mtp_path, int threads_per_block, const double* basic,
                          double* moments, double* dmoments, double* energy_part);
+
+/*
+ * Device neighbour rows with a cell list (positions d_pos [natoms][3] on the
+ * device, cell9 = the three lattice vectors as rows, host).  For every atom,
+ * the slots hold every periodic image within `cutoff`: owner index (d_js),
+ * image code (d_image, for mtp_pack_rij_device), species (d_jtypes), and the
+ * count (d_counts); unused slots get index -1 and species -1.  Rows longer
+ * than nbr_stride are truncated and reported as MTP_E_CAPACITY by
+ * mtp_sync_status (the reference drops such neighbours silently,
+ * pair_jax_mtp.cpp:132).  Each cell edge must be at least `cutoff` long.
+ * Replaces the host packing of pair_jax_mtp.cpp:110-167 for device-resident MD.
+ */
+int mtp_neighbors_device(mtp_handle* h, int natoms, const double* d_pos, const double* cell9,
+                         const int* d_types, double cutoff, int nbr_stride, int* d_js, int* d_image,
+                         int* d_jtypes, int* d_counts);
+
+/* r_ij = x_j - x_i + image . cell for the rows of mtp_neighbors_device (device). */
+int mtp_pack_rij_device(mtp_handle* h, int natoms, int nbr_stride, const double* d_pos, const double* cell9,
+                        const int* d_js, const int* d_image, const int* d_counts, double* d_rijs);
+
+/* Velocity Verlet in LAMMPS 'metal' units (A, ps, eV, amu): stage 1 = half kick
+ * + drift, stage 2 = half kick.  masses [species] in amu (host). */
+int mtp_verlet_device(mtp_handle* h, int natoms, double* d_x, double* d_v, const double* d_f, const int* d_types,
+                      const double* masses, int nmasses, double dt, int stage);
+
+/* Time the evaluation kernel with CUDA events on the handle's stream:
+ * enable = 1 starts accumulating, mtp_profile_read returns the total kernel
+ * milliseconds and launch count since enabling (synchronises). */
+int mtp_profile(mtp_handle* h, int enable);
+int mtp_profile_read(mtp_handle* h, double* eval_ms, int* eval_launches);
 
 /* Peak FP64 / FP32 FMA throughput of device 0 measured by an FMA-chain kernel
  * (TFLOP/s, an FMA counted as 2 flops).  Used for the roofline. */

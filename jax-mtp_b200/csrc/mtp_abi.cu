@@ -19,6 +19,7 @@
 
 #include "../../include/mtp_b200.h"
 #include "mtp_launch.hpp"
+#include "mtp_md.hpp"
 #include "mtp_model.hpp"
 #include "mtp_train.hpp"
 
@@ -71,6 +72,15 @@ struct mtp_handle {
   double* h_tot = nullptr;   // pinned [7]
   int* h_err = nullptr;      // pinned [1]
   TrainWorkspace train;
+  CellScratch cells;
+  // launch decisions by (requested lanes, stride, precision): no occupancy
+  // queries after the first call, so later calls can be graph-captured
+  struct LaunchChoice { int lanes, bps; bool vglobal; size_t smem; };
+  std::map<long long, LaunchChoice> launch_cache;
+  // profiling of the evaluation kernel
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+  int prof_used = 0;
   // statistics
   long long calls = 0;
   double total_ms = 0.0;
@@ -186,6 +196,12 @@ void free_handle(mtp_handle* h) {
   F(h->d_in_cnt); F(h->d_in_ptr); F(h->d_in_cursor); F(h->d_in_slot); F(h->d_blk);
   F(h->d_partials); F(h->d_tot); F(h->d_err); F(h->d_cfg_ptr); F(h->d_vscratch);
   train_free(h->train);
+  F(h->cells.cell); F(h->cells.img); F(h->cells.cnt); F(h->cells.ptr); F(h->cells.cursor); F(h->cells.atoms);
+  F(h->cells.blk);
+  for (auto& ev : h->prof_events) {
+    cudaEventDestroy(ev.first);
+    cudaEventDestroy(ev.second);
+  }
   if (h->h_tot) cudaFreeHost(h->h_tot);
   if (h->h_err) cudaFreeHost(h->h_err);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -201,6 +217,34 @@ int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, 
   DeviceSchedule* ds = nullptr;
   bool vglobal = false;
   int bps = 0;
+  const long long key = (static_cast<long long>(h->threads) << 40) | (static_cast<long long>(stride) << 8) |
+                        (fp64 ? 1 : 0) | (h->blocks_per_sm << 1);
+  auto hit = h->launch_cache.find(key);
+  if (hit != h->launch_cache.end()) {
+    const auto& c = hit->second;
+    int st = get_schedule(h, c.lanes, &ds);
+    if (st != MTP_OK) return st;
+    long long blocks = std::max(1LL, std::min<long long>(static_cast<long long>(c.bps) * h->sm_count, natoms));
+    if (c.vglobal) {
+      const size_t need = static_cast<size_t>(blocks) * ds->sched.v_size * (fp64 ? sizeof(double) : sizeof(float));
+      if (need > h->vscratch_bytes) {
+        if (h->d_vscratch) cudaFree(h->d_vscratch);
+        h->d_vscratch = nullptr;
+        h->vscratch_bytes = 0;
+        MTP_CUDA(h, cudaMalloc(&h->d_vscratch, need));
+        h->vscratch_bytes = need;
+      }
+    }
+    *ds_out = ds;
+    *blocks_out = static_cast<int>(blocks);
+    *vglobal_out = c.vglobal;
+    h->last_threads = c.lanes;
+    h->last_blocks = static_cast<int>(blocks);
+    h->last_bps = c.bps;
+    h->last_vglobal = c.vglobal;
+    h->last_smem = c.smem;
+    return MTP_OK;
+  }
   for (int alt : {lanes, 256, 128}) {
     if (alt > lanes) continue;
     int st = get_schedule(h, alt, &ds);
@@ -241,6 +285,7 @@ int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, 
   h->last_bps = bps;
   h->last_vglobal = vglobal;
   h->last_smem = eval_smem_bytes(make_model(h, *ds), stride, lanes, fp64, vglobal);
+  h->launch_cache[key] = mtp_handle::LaunchChoice{lanes, bps, vglobal, h->last_smem};
   return MTP_OK;
 }
 
@@ -270,7 +315,21 @@ int run_device(mtp_handle* h, int natoms, int stride, const int* itypes, const d
     MTP_CUDA(h, launch_incoming(natoms, stride, js, jtypes, counts, h->d_in_cnt, h->d_in_ptr, h->d_in_cursor,
                                 h->d_in_slot, h->d_blk, h->stream));
   }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (h->profiling) {
+    if (h->prof_used == static_cast<int>(h->prof_events.size())) {
+      cudaEvent_t a, b;
+      MTP_CUDA(h, cudaEventCreate(&a));
+      MTP_CUDA(h, cudaEventCreate(&b));
+      h->prof_events.push_back({a, b});
+    }
+    e0 = h->prof_events[h->prof_used].first;
+    e1 = h->prof_events[h->prof_used].second;
+    ++h->prof_used;
+    MTP_CUDA(h, cudaEventRecord(e0, h->stream));
+  }
   MTP_CUDA(h, launch_eval(md, io, h->last_threads, blocks, fp64, vglobal, h->stream));
+  if (e1) MTP_CUDA(h, cudaEventRecord(e1, h->stream));
   MTP_CUDA(h, launch_force_gather(natoms, stride, rijs, counts, h->d_G, h->d_in_ptr, h->d_in_slot, forces,
                                   h->d_wown, vatom, h->stream));
   return MTP_OK;
@@ -432,7 +491,13 @@ const char* mtp_last_error(const mtp_handle* h) { return h ? h->err.c_str() : g_
 
 int mtp_set_stream(mtp_handle* h, void* s) {
   if (!h) return MTP_E_INVALID;
-  h->stream = s ? static_cast<cudaStream_t>(s) : h->own_stream;
+  h->stream = static_cast<cudaStream_t>(s);
+  return MTP_OK;
+}
+
+int mtp_use_own_stream(mtp_handle* h) {
+  if (!h) return MTP_E_INVALID;
+  h->stream = h->own_stream;
   return MTP_OK;
 }
 
@@ -672,6 +737,101 @@ int mtp_adjoint_batch_device(mtp_handle* h, int natoms, int stride, int nconfig,
   if (!err.empty()) return fail(h, MTP_E_CAPACITY, err);
   if (ce != cudaSuccess) return cuda_fail(h, ce, "adjoint");
   h->calls++;
+  return MTP_OK;
+}
+
+namespace {
+int ensure_cells(mtp_handle* h, int n, int ncell) {
+  CellScratch& c = h->cells;
+  if (n > c.n_cap) {
+    if (c.cell) cudaFree(c.cell);
+    if (c.img) cudaFree(c.img);
+    if (c.atoms) cudaFree(c.atoms);
+    c.cell = c.img = c.atoms = nullptr;
+    c.n_cap = 0;
+    MTP_CUDA(h, dalloc(&c.cell, n));
+    MTP_CUDA(h, dalloc(&c.img, 3 * static_cast<size_t>(n)));
+    MTP_CUDA(h, dalloc(&c.atoms, n));
+    c.n_cap = n;
+  }
+  if (ncell > c.cell_cap) {
+    if (c.cnt) cudaFree(c.cnt);
+    if (c.ptr) cudaFree(c.ptr);
+    if (c.cursor) cudaFree(c.cursor);
+    if (c.blk) cudaFree(c.blk);
+    c.cnt = c.ptr = c.cursor = c.blk = nullptr;
+    c.cell_cap = 0;
+    MTP_CUDA(h, dalloc(&c.cnt, ncell));
+    MTP_CUDA(h, dalloc(&c.ptr, ncell + 1));
+    MTP_CUDA(h, dalloc(&c.cursor, ncell));
+    MTP_CUDA(h, dalloc(&c.blk, ncell / 1024 + 2));
+    c.cell_cap = ncell;
+  }
+  return MTP_OK;
+}
+}  // namespace
+
+int mtp_neighbors_device(mtp_handle* h, int natoms, const double* d_pos, const double* cell9, const int* d_types,
+                         double cutoff, int stride, int* d_js, int* d_image, int* d_jtypes, int* d_counts) {
+  if (!h) return MTP_E_INVALID;
+  if (natoms < 0 || stride <= 0 || !(cutoff > 0.0) || !cell9) return fail(h, MTP_E_INVALID, "bad arguments");
+  if (natoms > 0 && (!d_pos || !d_types || !d_js || !d_image || !d_jtypes || !d_counts))
+    return fail(h, MTP_E_INVALID, "null pointer");
+  Box b;
+  if (!make_box(cell9, cutoff, b)) return fail(h, MTP_E_INVALID, "singular cell");
+  if (b.nc[0] < 1 || b.nc[1] < 1 || b.nc[2] < 1)
+    return fail(h, MTP_E_INVALID, "cell thinner than the cutoff: build these rows on the host");
+  const long long ncell = static_cast<long long>(b.nc[0]) * b.nc[1] * b.nc[2];
+  if (ncell > (1LL << 28)) return fail(h, MTP_E_CAPACITY, "too many cells");
+  int st = ensure_cells(h, natoms, static_cast<int>(ncell));
+  if (st != MTP_OK) return st;
+  MTP_CUDA(h, launch_neighbors(natoms, d_pos, b, d_types, cutoff, stride, d_js, d_image, d_jtypes, d_counts,
+                               h->cells, h->d_err, h->stream));
+  return MTP_OK;
+}
+
+int mtp_pack_rij_device(mtp_handle* h, int natoms, int stride, const double* d_pos, const double* cell9,
+                        const int* d_js, const int* d_image, const int* d_counts, double* d_rijs) {
+  if (!h) return MTP_E_INVALID;
+  if (natoms < 0 || stride <= 0 || !cell9) return fail(h, MTP_E_INVALID, "bad arguments");
+  if (natoms > 0 && (!d_pos || !d_js || !d_image || !d_counts || !d_rijs)) return fail(h, MTP_E_INVALID, "null pointer");
+  Box b;
+  if (!make_box(cell9, 1.0, b)) return fail(h, MTP_E_INVALID, "singular cell");
+  MTP_CUDA(h, launch_pack_rij(natoms, stride, d_pos, b, d_js, d_image, d_counts, d_rijs, h->stream));
+  return MTP_OK;
+}
+
+int mtp_verlet_device(mtp_handle* h, int natoms, double* d_x, double* d_v, const double* d_f, const int* d_types,
+                      const double* masses, int nmasses, double dt, int stage) {
+  if (!h) return MTP_E_INVALID;
+  if (natoms < 0 || !masses || nmasses <= 0 || nmasses > kMaxMdSpecies || (stage != 1 && stage != 2))
+    return fail(h, MTP_E_INVALID, "bad arguments");
+  VerletParams p{};
+  p.dt = dt;
+  p.ftm2v = 1.0 / 1.0364269e-4;   // LAMMPS 'metal' force->ftm2v
+  for (int t = 0; t < kMaxMdSpecies; ++t) p.inv_mass[t] = 1.0 / masses[std::min(t, nmasses - 1)];
+  MTP_CUDA(h, launch_verlet(natoms, d_x, d_v, d_f, d_types, p, stage, h->stream));
+  return MTP_OK;
+}
+
+int mtp_profile(mtp_handle* h, int enable) {
+  if (!h) return MTP_E_INVALID;
+  h->profiling = enable != 0;
+  h->prof_used = 0;
+  return MTP_OK;
+}
+
+int mtp_profile_read(mtp_handle* h, double* ms, int* launches) {
+  if (!h || !ms || !launches) return MTP_E_INVALID;
+  MTP_CUDA(h, cudaStreamSynchronize(h->stream));
+  double tot = 0.0;
+  for (int i = 0; i < h->prof_used; ++i) {
+    float x = 0.f;
+    MTP_CUDA(h, cudaEventElapsedTime(&x, h->prof_events[i].first, h->prof_events[i].second));
+    tot += x;
+  }
+  *ms = tot;
+  *launches = h->prof_used;
   return MTP_OK;
 }
 

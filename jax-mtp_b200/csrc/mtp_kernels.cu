@@ -1,6 +1,7 @@
 // mtp_kernels.cu - evaluation-kernel instantiations and the supporting kernels:
 // incoming-slot lists, deterministic force gather, fixed-order reductions.
 #include "mtp_launch.hpp"
+#include "mtp_md.hpp"
 
 namespace mtp {
 
@@ -39,9 +40,15 @@ int eval_blocks_per_sm(const DevModel& md, int n_pad, int threads, bool fp64, bo
 template <typename T, bool G>
 static cudaError_t launch_eval_t(const DevModel& md, const DevIO& io, int threads, int blocks, size_t bytes,
                                  cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(k_mtp_eval<T, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(bytes));
-  if (e != cudaSuccess) return e;
+  // raise the dynamic shared-memory limit only when a larger size is needed,
+  // so steady-state launches make no attribute calls (CUDA-graph capture)
+  static size_t granted = 0;
+  if (bytes > granted) {
+    cudaError_t e = cudaFuncSetAttribute(k_mtp_eval<T, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(bytes));
+    if (e != cudaSuccess) return e;
+    granted = bytes;
+  }
   k_mtp_eval<T, G><<<blocks, threads, bytes, st>>>(md, io);
   return cudaGetLastError();
 }
@@ -149,6 +156,16 @@ __global__ void k_scan_add(int n, int* out, const int* block_off) {
   if (i < n) out[i] += block_off[blockIdx.x];
 }
 
+// out[0..n) = exclusive prefix sums of in, out[n] = total; blk holds n/1024 + 1 ints.
+cudaError_t scan_exclusive(int n, const int* in, int* out, int* blk, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int nb = (n + 1023) / 1024;
+  k_scan_blocks<<<nb, 1024, 0, st>>>(n, in, out, blk);
+  k_scan_totals<<<1, 1024, 0, st>>>(nb, blk, out + n);
+  k_scan_add<<<nb, 1024, 0, st>>>(n, out, blk);
+  return cudaGetLastError();
+}
+
 __global__ void k_fill_incoming(int natoms, int stride, const int* js, const int* jtypes, const int* counts,
                                 const int* in_ptr, int* in_cursor, int* in_slot) {
   const size_t n = static_cast<size_t>(natoms) * stride;
@@ -189,10 +206,8 @@ cudaError_t launch_incoming(int natoms, int stride, const int* js, const int* jt
   const size_t n = static_cast<size_t>(natoms) * stride;
   const int gb = static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 32));
   k_count_incoming<<<gb, 256, 0, st>>>(natoms, stride, js, jtypes, counts, in_cnt);
-  const int nb = (natoms + 1023) / 1024;
-  k_scan_blocks<<<nb, 1024, 0, st>>>(natoms, in_cnt, in_ptr, block_tmp);
-  k_scan_totals<<<1, 1024, 0, st>>>(nb, block_tmp, in_ptr + natoms);
-  k_scan_add<<<nb, 1024, 0, st>>>(natoms, in_ptr, block_tmp);
+  cudaError_t e = scan_exclusive(natoms, in_cnt, in_ptr, block_tmp, st);
+  if (e != cudaSuccess) return e;
   k_fill_incoming<<<gb, 256, 0, st>>>(natoms, stride, js, jtypes, counts, in_ptr, in_cursor, in_slot);
   k_sort_incoming<<<(natoms + 127) / 128, 128, 0, st>>>(natoms, in_ptr, in_slot);
   return cudaGetLastError();

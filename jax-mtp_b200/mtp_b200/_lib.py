@@ -30,6 +30,7 @@ SIGNATURES = {
     "mtp_destroy": (None, [_P]),
     "mtp_last_error": (ctypes.c_char_p, [_P]),
     "mtp_set_stream": (_I, [_P, _P]),
+    "mtp_use_own_stream": (_I, [_P]),
     "mtp_get_info": (_I, [_P, _P]),
     "mtp_set_coeffs": (_I, [_P, _P, _P, _P]),
     "mtp_execute_potential": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _D, _P, _P, _P]),
@@ -43,6 +44,11 @@ SIGNATURES = {
     "mtp_parse_info": (_I, [ctypes.c_char_p, _P, ctypes.c_char_p, _I]),
     "mtp_schedule_emulate": (_I, [ctypes.c_char_p, _I, _P, _P, _P, _P]),
     "mtp_measure_fma_peak": (_I, [ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "mtp_neighbors_device": (_I, [_P, _I, _P, _P, _P, _D, _I, _P, _P, _P, _P]),
+    "mtp_pack_rij_device": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "mtp_verlet_device": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _D, _I]),
+    "mtp_profile": (_I, [_P, _I]),
+    "mtp_profile_read": (_I, [_P, ctypes.POINTER(_D), ctypes.POINTER(_I)]),
 }
 
 _lib = None

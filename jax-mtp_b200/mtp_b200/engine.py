@@ -90,7 +90,11 @@ class MTPEngine:
         check(lib().mtp_set_coeffs(self._h, _ptr(sp), _ptr(mo), _ptr(ra)), self._h)
 
     def set_stream(self, stream_handle: int) -> None:
+        """Work on this cudaStream_t (0 = the legacy default stream, as torch's default)."""
         check(lib().mtp_set_stream(self._h, ctypes.c_void_p(stream_handle)), self._h)
+
+    def use_own_stream(self) -> None:
+        check(lib().mtp_use_own_stream(self._h), self._h)
 
     def set_launch(self, threads: int, blocks_per_sm: int = 0) -> None:
         check(lib().mtp_set_launch(self._h, int(threads), int(blocks_per_sm)), self._h)
@@ -253,3 +257,59 @@ def measure_fma_peak():
     f = ctypes.c_double()
     check(lib().mtp_measure_fma_peak(ctypes.byref(d), ctypes.byref(f)))
     return d.value, f.value
+
+
+# ----------------------------------------------------------------------------
+# device MD helpers (bound as methods below)
+# ----------------------------------------------------------------------------
+def _tp(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _neighbors_device(self, pos, cell, types, cutoff: float, stride: int, js, image, jtypes, counts, stream=None):
+    """Device cell-list rows (see mtp_neighbors_device)."""
+    import torch
+    st = torch.cuda.current_stream(pos.device) if stream is None else stream
+    self.set_stream(st.cuda_stream)
+    c9 = _c(np.asarray(cell, dtype=np.float64).reshape(9), np.float64)
+    code = lib().mtp_neighbors_device(self._h, int(pos.shape[0]), _tp(pos), _ptr(c9), _tp(types), float(cutoff),
+                                      int(stride), _tp(js), _tp(image), _tp(jtypes), _tp(counts))
+    check(code, self._h)
+
+
+def _pack_rij_device(self, pos, cell, js, image, counts, rijs, stream=None):
+    import torch
+    st = torch.cuda.current_stream(pos.device) if stream is None else stream
+    self.set_stream(st.cuda_stream)
+    c9 = _c(np.asarray(cell, dtype=np.float64).reshape(9), np.float64)
+    code = lib().mtp_pack_rij_device(self._h, int(pos.shape[0]), int(js.shape[1]), _tp(pos), _ptr(c9), _tp(js),
+                                     _tp(image), _tp(counts), _tp(rijs))
+    check(code, self._h)
+
+
+def _verlet_device(self, x, v, f, types, masses, dt: float, stage: int, stream=None):
+    import torch
+    st = torch.cuda.current_stream(x.device) if stream is None else stream
+    self.set_stream(st.cuda_stream)
+    m = _c(masses, np.float64)
+    code = lib().mtp_verlet_device(self._h, int(x.shape[0]), _tp(x), _tp(v), _tp(f), _tp(types), _ptr(m), len(m),
+                                   float(dt), int(stage))
+    check(code, self._h)
+
+
+def _profile(self, enable: bool) -> None:
+    check(lib().mtp_profile(self._h, 1 if enable else 0), self._h)
+
+
+def _profile_read(self):
+    ms = ctypes.c_double()
+    n = ctypes.c_int()
+    check(lib().mtp_profile_read(self._h, ctypes.byref(ms), ctypes.byref(n)), self._h)
+    return ms.value, n.value
+
+
+MTPEngine.neighbors_device = _neighbors_device
+MTPEngine.pack_rij_device = _pack_rij_device
+MTPEngine.verlet_device = _verlet_device
+MTPEngine.profile = _profile
+MTPEngine.profile_read = _profile_read

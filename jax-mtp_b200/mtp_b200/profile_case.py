@@ -1,0 +1,61 @@
+"""A bounded evaluation case for profilers (ncu) and quick timing.
+
+    python -m mtp_b200.profile_case --potential <file.mtp> --reps 32 --precision mixed --calls 3
+
+Builds an fcc a=3.6 A crystal of reps^3 cells (4 reps^3 atoms) with thermal
+displacements, device neighbour rows (cutoff max_dist + 0.3 A), and calls the
+evaluation `--calls` times; prints the evaluation-kernel time per call
+measured with CUDA events.  reps=32 gives 131,072 atoms and 200 MB of r_ij,
+larger than the 126 MB L2, while staying a few GB on the device.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+
+import numpy as np
+import torch
+
+from . import synth
+from .engine import MTPEngine
+from .mtp_file import read_mtp
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--potential", required=True)
+    ap.add_argument("--reps", type=int, default=32)
+    ap.add_argument("--stride", type=int, default=64)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--calls", type=int, default=3)
+    ap.add_argument("--threads", type=int, default=0)
+    a = ap.parse_args(argv)
+    pot = read_mtp(a.potential)
+    s = synth.config2_structure(a.reps)
+    s.types = s.types % pot.species_count
+    dev = torch.device("cuda")
+    N = s.natoms
+    with MTPEngine(a.potential, N, a.stride, precision=a.precision) as eng:
+        if a.threads:
+            eng.set_launch(a.threads)
+        x = torch.as_tensor(s.positions, device=dev)
+        t = torch.as_tensor(s.types, device=dev)
+        js = torch.empty((N, a.stride), dtype=torch.int32, device=dev)
+        im, jt = torch.empty_like(js), torch.empty_like(js)
+        cnt = torch.empty(N, dtype=torch.int32, device=dev)
+        rij = torch.empty((N, a.stride, 3), dtype=torch.float64, device=dev)
+        eng.neighbors_device(x, s.cell, t, pot.max_dist + 0.3, a.stride, js, im, jt, cnt)
+        eng.pack_rij_device(x, s.cell, js, im, cnt, rij)
+        eng.profile(True)
+        for k in range(a.calls):
+            eng.compute_device(t, rij, js, jt, cnt, reuse_neighbors=k > 0)
+        ms, n = eng.profile_read()
+        eng.sync_status()
+        print(json.dumps({"atoms": N, "precision": a.precision, "eval_ms_per_call": ms / max(1, n),
+                          "launch": eng.launch()}))
+
+
+if __name__ == "__main__":
+    main()

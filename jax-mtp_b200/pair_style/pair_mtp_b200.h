@@ -1,0 +1,66 @@
+/* ----------------------------------------------------------------------
+   pair_style jax/mtp on the B200 MTP engine (C ABI include/mtp_b200.h)
+
+   Keeps the reference pair style's surface (pair_style_files/pair_jax_mtp.h,
+   pair_jax_mtp.cpp:228-282):
+
+     pair_style jax/mtp <potential.mtp> MAX_ATOMS MAX_ATOMS_PER_NEIGHBOR MTP_CUTOFF [DEBUG_LEVEL] [fp64|mixed]
+     pair_coeff * *
+
+   The first argument is the .mtp potential itself (the reference took a
+   jax.export .bin compiled from it; a .bin is rejected with a clear error).
+   Needs atom IDs, a full neighbour list, and one MPI rank (as the reference).
+------------------------------------------------------------------------- */
+
+#ifdef PAIR_CLASS
+// clang-format off
+PairStyle(jax/mtp,PairMTPB200);
+// clang-format on
+#else
+
+#ifndef LMP_PAIR_MTP_B200_H
+#define LMP_PAIR_MTP_B200_H
+
+#include <vector>
+
+#include "pair.h"
+
+struct mtp_handle;
+
+namespace LAMMPS_NS {
+
+class PairMTPB200 : public Pair {
+ public:
+  PairMTPB200(class LAMMPS *);
+  ~PairMTPB200() override;
+
+  void compute(int, int) override;
+  void settings(int, char **) override;
+  void coeff(int, char **) override;
+  double init_one(int, int) override;
+  void init_style() override;
+
+  // statistics, for a driver's summary
+  long long calls() const { return total_calls; }
+
+ protected:
+  void allocate();
+  void grow_buffers();
+
+  char *mtp_path;
+  double cutoff;
+  int max_atoms, max_nbr, debug_level, precision;
+  mtp_handle *handle;
+  long long total_calls;
+
+  // persistent flat buffers [max_atoms][max_nbr] (no per-step allocation)
+  std::vector<double> rij;
+  std::vector<int> js, jtypes, counts, itypes;
+  std::vector<double> fbuf, ebuf, vbuf;
+  std::vector<int> tag_to_local;
+};
+
+}    // namespace LAMMPS_NS
+
+#endif
+#endif

@@ -75,9 +75,12 @@ struct DevIO {
 };
 
 // Shared-memory carve of the evaluation kernel.
+// Depth of the per-thread prefetch ring of lane-program entries.
+constexpr int kRing = 8;
+
 struct SmemLayout {
   int pws;        // stride of a power row (3 (D+1), rounded up to odd)
-  size_t v, rad, u, f, fp, pw, slot, abc, mk, red, cnt, total;
+  size_t v, rad, u, f, fp, pw, slot, abc, mk, red, cnt, ring, total;
 };
 
 template <typename T>
@@ -103,6 +106,7 @@ __host__ __device__ inline SmemLayout smem_layout(int v_size, int S, int R, int 
   L.mk = take(sizeof(int) * kMaxR * P);
   L.red = take(sizeof(double) * (threads / 32));
   L.cnt = take(sizeof(int) * (threads / 32 + 1));
+  L.ring = take(sizeof(uint2) * kRing * threads);
   L.total = (o + 15) & ~size_t(15);
   return L;
 }
@@ -112,15 +116,51 @@ __device__ __forceinline__ float dev_sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double dev_fma(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float dev_fma(float a, float b, float c) { return fmaf(a, b, c); }
 
-// Execute one lane program pass: acc += c * V[a] * V[b]; flush on STORE/ADD.
-template <typename T>
-__device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int steps, int lanes, int tid,
-                                         T* __restrict__ V) {
+// Asynchronous 8-byte global -> shared copy (cp.async, cached in L1).
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Stream one lane program pass through a per-thread ring of kRing entries in
+// shared memory: entry e lives in ring slot e % kRing and is requested
+// kRing - 1 steps before it is used, so the L2 latency of the program (the
+// whole schedule is ~1 MB at level 24 and cannot stay in L1) overlaps the
+// arithmetic of the preceding steps.  The ring column of a thread is written
+// and read by that thread only.
+template <typename Body>
+__device__ __forceinline__ void stream_pass(const uint2* __restrict__ ent, int steps, int lanes, int tid,
+                                            uint2* __restrict__ ring, Body& body) {
   const uint2* p = ent + tid;
-  T acc = T(0);
-#pragma unroll 4
+#pragma unroll
+  for (int k = 0; k < kRing; ++k) {
+    if (k < steps) cp_async8(ring + k * lanes + tid, p + static_cast<size_t>(k) * lanes);
+    cp_async_commit();
+  }
   for (int s = 0; s < steps; ++s) {
-    uint2 e = __ldg(p + static_cast<size_t>(s) * lanes);
+    if (s >= 1) {
+      const int nx = s + kRing - 1;   // refills the slot read in the previous step
+      if (nx < steps) cp_async8(ring + (nx % kRing) * lanes + tid, p + static_cast<size_t>(nx) * lanes);
+      cp_async_commit();
+    }
+    cp_async_wait<kRing - 1>();
+    const uint2 e = ring[(s % kRing) * lanes + tid];
+    body(e);
+  }
+  cp_async_wait<0>();
+}
+
+// acc += c * V[a] * V[b]; on STORE/ADD write the accumulator and restart.
+template <typename T>
+struct PlainBody {
+  T* V;
+  T acc;
+  __device__ __forceinline__ void operator()(const uint2 e) {
     const T c = static_cast<T>(e.y >> 18);
     acc = dev_fma(c * V[e.x & 0xFFFFu], V[e.x >> 16], acc);
     const uint32_t op = (e.y >> 16) & 3u;
@@ -131,6 +171,14 @@ __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int step
       acc = T(0);
     }
   }
+};
+
+// Execute one lane program pass with the plain arithmetic.
+template <typename T>
+__device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int steps, int lanes, int tid,
+                                         T* __restrict__ V, uint2* __restrict__ ring) {
+  PlainBody<T> body{V, T(0)};
+  stream_pass(ent, steps, lanes, tid, ring, body);
 }
 
 // Deterministic block sum of one double per thread (valid in thread 0).
@@ -171,6 +219,7 @@ __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
   int* sMk = reinterpret_cast<int*>(smem + L.mk);
   double* sRed = reinterpret_cast<double*>(smem + L.red);
   int* sCnt = reinterpret_cast<int*>(smem + L.cnt);
+  uint2* sRing = reinterpret_cast<uint2*>(smem + L.ring);
 
   const int S = md.S, R = md.R, K = md.K, P = md.P, D1 = md.D + 1, pws = L.pws;
   // per-block constants
@@ -333,7 +382,7 @@ __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
 
     // ---- T: forward contraction passes ----------------------------------
     for (int ps = 0; ps < md.nfwd; ++ps) {
-      run_pass<T>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, V);
+      run_pass<T>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, V, sRing);
       __syncthreads();
     }
     // energy: E_i = xi[t_i] + sum_alpha theta_alpha m[map_alpha] in FP64
@@ -349,7 +398,7 @@ __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
 
     // ---- R: reverse passes (dE/dm) ---------------------------------------
     for (int ps = 0; ps < md.nrev; ++ps) {
-      run_pass<T>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, V);
+      run_pass<T>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, V, sRing);
       __syncthreads();
     }
 

@@ -7,7 +7,7 @@ namespace mtp {
 
 struct TrainSmem {
   int pws;
-  size_t v, rad, u, du, f, fp, phi, phip, pw, A, Bv, jt, abc, mk, gth, gxi, grad, red, cnt, total;
+  size_t v, rad, u, du, f, fp, phi, phip, pw, A, Bv, jt, abc, mk, gth, gxi, grad, red, cnt, ring, total;
 };
 
 template <typename T>
@@ -41,19 +41,18 @@ __host__ __device__ inline TrainSmem train_layout(int v_size, int S, int R, int 
   L.grad = take(sizeof(double) * S * S * R * K);
   L.red = take(sizeof(double) * (threads / 32));
   L.cnt = take(sizeof(int) * (threads / 32 + 1));
+  L.ring = take(sizeof(uint2) * kRing * threads);
   L.total = (o + 15) & ~size_t(15);
   return L;
 }
 
 // Forward pass on duals: (m3, dm3) += c * (m1 m2, dm1 m2 + m1 dm2).
 template <typename T>
-__device__ __forceinline__ void run_pass_dual_fwd(const uint2* __restrict__ ent, int steps, int lanes, int tid,
-                                                  T* __restrict__ V, int H) {
-  const uint2* p = ent + tid;
-  T acc = T(0), tac = T(0);
-#pragma unroll 2
-  for (int s = 0; s < steps; ++s) {
-    uint2 e = __ldg(p + static_cast<size_t>(s) * lanes);
+struct DualFwdBody {
+  T* V;
+  int H;
+  T acc, tac;
+  __device__ __forceinline__ void operator()(const uint2 e) {
     const T c = static_cast<T>(e.y >> 18);
     const uint32_t a = e.x & 0xFFFFu, b = e.x >> 16;
     const T va = V[a], vb = V[b], ta = V[a + H], tb = V[b + H];
@@ -73,18 +72,16 @@ __device__ __forceinline__ void run_pass_dual_fwd(const uint2* __restrict__ ent,
       tac = T(0);
     }
   }
-}
+};
 
 // Reverse pass on duals (entries dst = adj[s], a = adj[t], b = m[o]):
 //   lambda_s += c (lambda_t m_o + tau_t dm_o),  tau_s += c tau_t m_o.
 template <typename T>
-__device__ __forceinline__ void run_pass_dual_rev(const uint2* __restrict__ ent, int steps, int lanes, int tid,
-                                                  T* __restrict__ V, int H) {
-  const uint2* p = ent + tid;
-  T acc = T(0), tac = T(0);
-#pragma unroll 2
-  for (int s = 0; s < steps; ++s) {
-    uint2 e = __ldg(p + static_cast<size_t>(s) * lanes);
+struct DualRevBody {
+  T* V;
+  int H;
+  T acc, tac;
+  __device__ __forceinline__ void operator()(const uint2 e) {
     const T c = static_cast<T>(e.y >> 18);
     const uint32_t a = e.x & 0xFFFFu, b = e.x >> 16;
     const T la = V[a], ta = V[a + H], mb = V[b], tb = V[b + H];
@@ -104,7 +101,7 @@ __device__ __forceinline__ void run_pass_dual_rev(const uint2* __restrict__ ent,
       tac = T(0);
     }
   }
-}
+};
 
 template <typename T, bool kVGlobal>
 __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, int n_pad, void* vscratch,
@@ -132,6 +129,7 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
   double* gXi = reinterpret_cast<double*>(smem + L.gxi);
   double* gRad = reinterpret_cast<double*>(smem + L.grad);
   int* sCnt = reinterpret_cast<int*>(smem + L.cnt);
+  uint2* sRing = reinterpret_cast<uint2*>(smem + L.ring);
   const int pws = L.pws;
   const int nrad = S * S * R * K;
 
@@ -354,7 +352,8 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
 
     // ---- dual forward tree --------------------------------------------------
     for (int ps = 0; ps < md.nfwd; ++ps) {
-      run_pass_dual_fwd<T>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, V, H);
+      DualFwdBody<T> body{V, H, T(0), T(0)};
+      stream_pass(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, sRing, body);
       __syncthreads();
     }
     for (int a = tid; a < md.Sa; a += NT) {
@@ -365,7 +364,8 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
 
     // ---- dual reverse tree ---------------------------------------------------
     for (int ps = 0; ps < md.nrev; ++ps) {
-      run_pass_dual_rev<T>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, V, H);
+      DualRevBody<T> body{V, H, T(0), T(0)};
+      stream_pass(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, sRing, body);
       __syncthreads();
     }
 

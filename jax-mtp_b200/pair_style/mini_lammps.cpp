@@ -87,6 +87,7 @@ void build_ghosts(Sim& s, double rcut) {
     const int o = s.ghost_owner[g], k = s.nlocal + g;
     s.type[k] = s.type[o];
     s.tag[k] = s.tag[o];
+    for (int a = 0; a < 3; ++a) s.xbuf[3 * k + a] = s.xbuf[3 * o + a] + s.ghost_shift[3 * g + a];
   }
   set_ptrs(s);
 }

@@ -210,6 +210,21 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------------------------
+def max_over_ranks(ms: float, dist, device) -> float:
+    """The job time is the slowest rank's (every rank runs one replica)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t[0])
+
+
+def job_value(atoms_per_rank: int, world: int, steps: int, ms: float) -> float:
+    """Whole-job atom-steps/s: all replicas' atoms x steps over the slowest rank's time."""
+    return world * atoms_per_rank * steps / (ms * 1e-3)
+
+
 def time_md(md, steps: int, warmup: int, dist, device, sampler=None):
     import torch
     md.run(warmup, graphs=True)
@@ -228,11 +243,8 @@ def time_md(md, steps: int, warmup: int, dist, device, sampler=None):
     torch.cuda.synchronize(device)
     if sampler is not None:
         sampler.__exit__()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, device)
     if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t[0])
         dist.barrier()
     return ms
 
@@ -317,8 +329,8 @@ def run_ours(args):
     # drift over the timed run (energy per atom)
     fp64_peak, fp32_peak = measure_fma_peak()
 
-    value = world * N * args.steps / (results["mixed"]["ms"] * 1e-3)
-    value64 = world * N * args.steps / (results["fp64"]["ms"] * 1e-3)
+    value = job_value(N, world, args.steps, results["mixed"]["ms"])
+    value64 = job_value(N, world, args.steps, results["fp64"]["ms"])
     k_mixed = results["mixed"]["eval_ms_per_launch"] * 1e-3
     k_64 = results["fp64"]["eval_ms_per_launch"] * 1e-3
     achieved = flops / k_mixed / 1e12

@@ -182,12 +182,15 @@ int mtp_adjoint_batch_device(mtp_handle* h, int natoms, int nbr_stride, int ncon
                              const double* d_gS, double* d_gspecies, double* d_gmoment,
                              double* d_gradial);
 
-/* Launch shape of the evaluation kernel: threads per block (128/256/512) and
- * blocks per SM (0 = as many as fit).  Used by the autotuner. */
-int mtp_set_launch(mtp_handle* h, int threads_per_block, int blocks_per_sm);
+/* Launch shape of the evaluation kernel: threads per block (128/256/512),
+ * blocks per SM (0 = as many as fit) and atoms evaluated together per block
+ * (0 = chosen by occupancy, or 1/2/4; FP64 supports 1/2).  Used by the
+ * autotuner. */
+int mtp_set_launch(mtp_handle* h, int threads_per_block, int blocks_per_sm, int atoms_per_block);
 
-/* Last evaluation kernel's launch: out4 = threads, blocks, dynamic shared bytes, blocks per SM. */
-int mtp_get_launch(const mtp_handle* h, int* out4);
+/* Last evaluation kernel's launch: out5 = threads, blocks, dynamic shared bytes,
+ * blocks per SM, atoms per block. */
+int mtp_get_launch(const mtp_handle* h, int* out5);
 
 /*
  * Parse an .mtp file on the host only (no device needed) and report its

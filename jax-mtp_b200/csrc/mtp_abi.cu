@@ -75,7 +75,9 @@ struct mtp_handle {
   CellScratch cells;
   // launch decisions by (requested lanes, stride, precision): no occupancy
   // queries after the first call, so later calls can be graph-captured
-  struct LaunchChoice { int lanes, bps; bool vglobal; size_t smem; };
+  struct LaunchChoice { int lanes, bps; bool vglobal; size_t smem; int A; };
+  int apb = 0;          // requested atoms per block (0: chosen by occupancy)
+  int last_apb = 1;
   std::map<long long, LaunchChoice> launch_cache;
   // profiling of the evaluation kernel
   bool profiling = false;
@@ -208,67 +210,69 @@ void free_handle(mtp_handle* h) {
   delete h;
 }
 
-// Launch shape for the evaluation kernel at the current settings: the
-// requested lanes with the value space in shared memory, else fewer lanes,
-// else the value space in global memory.
+// Launch shape for the evaluation kernel.  Candidates are (lanes, atoms per
+// block) with the value space in shared memory; the one with the most atoms
+// in flight per SM (A x blocks/SM) wins, ties going to more warps.  When none
+// fits, the value space moves to global memory (A = 1).  Decisions are cached
+// per (request, stride, precision), so later calls make no occupancy queries.
 int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, int* blocks_out, bool fp64,
                 bool* vglobal_out) {
-  int lanes = h->threads;
-  DeviceSchedule* ds = nullptr;
-  bool vglobal = false;
-  int bps = 0;
-  const long long key = (static_cast<long long>(h->threads) << 40) | (static_cast<long long>(stride) << 8) |
-                        (fp64 ? 1 : 0) | (h->blocks_per_sm << 1);
+  const long long key = (static_cast<long long>(h->threads) << 40) | (static_cast<long long>(h->apb) << 36) |
+                        (static_cast<long long>(h->blocks_per_sm) << 28) | (static_cast<long long>(stride) << 2) |
+                        (fp64 ? 1 : 0);
   auto hit = h->launch_cache.find(key);
+  mtp_handle::LaunchChoice c{};
   if (hit != h->launch_cache.end()) {
-    const auto& c = hit->second;
-    int st = get_schedule(h, c.lanes, &ds);
-    if (st != MTP_OK) return st;
-    long long blocks = std::max(1LL, std::min<long long>(static_cast<long long>(c.bps) * h->sm_count, natoms));
-    if (c.vglobal) {
-      const size_t need = static_cast<size_t>(blocks) * ds->sched.v_size * (fp64 ? sizeof(double) : sizeof(float));
-      if (need > h->vscratch_bytes) {
-        if (h->d_vscratch) cudaFree(h->d_vscratch);
-        h->d_vscratch = nullptr;
-        h->vscratch_bytes = 0;
-        MTP_CUDA(h, cudaMalloc(&h->d_vscratch, need));
-        h->vscratch_bytes = need;
+    c = hit->second;
+  } else {
+    std::vector<int> lanes_c = {h->threads};
+    for (int alt : {256, 128})
+      if (alt < h->threads) lanes_c.push_back(alt);
+    std::vector<int> a_c;
+    if (h->apb > 0) a_c = {h->apb};
+    else if (fp64) a_c = {2, 1};
+    else a_c = {4, 2, 1};
+    int best = -1;
+    for (int lanes : lanes_c) {
+      DeviceSchedule* ds = nullptr;
+      int st = get_schedule(h, lanes, &ds);
+      if (st != MTP_OK) return st;
+      const DevModel md = make_model(h, *ds);
+      for (int A : a_c) {
+        if (!eval_variant_exists(fp64, false, A)) continue;
+        int bps = eval_blocks_per_sm(md, stride, lanes, fp64, false, A);
+        if (h->blocks_per_sm > 0) bps = std::min(bps, h->blocks_per_sm);
+        if (bps <= 0) continue;
+        const int score = (A * bps) * 1024 + bps * lanes / 32;
+        if (score > best) {
+          best = score;
+          c = mtp_handle::LaunchChoice{lanes, bps, false, 0, A};
+        }
       }
     }
-    *ds_out = ds;
-    *blocks_out = static_cast<int>(blocks);
-    *vglobal_out = c.vglobal;
-    h->last_threads = c.lanes;
-    h->last_blocks = static_cast<int>(blocks);
-    h->last_bps = c.bps;
-    h->last_vglobal = c.vglobal;
-    h->last_smem = c.smem;
-    return MTP_OK;
-  }
-  for (int alt : {lanes, 256, 128}) {
-    if (alt > lanes) continue;
-    int st = get_schedule(h, alt, &ds);
-    if (st != MTP_OK) return st;
-    bps = eval_blocks_per_sm(make_model(h, *ds), stride, alt, fp64, false);
-    if (bps > 0) {
-      lanes = alt;
-      break;
+    if (best < 0) {
+      DeviceSchedule* ds = nullptr;
+      int st = get_schedule(h, h->threads, &ds);
+      if (st != MTP_OK) return st;
+      int bps = eval_blocks_per_sm(make_model(h, *ds), stride, h->threads, fp64, true, 1);
+      if (h->blocks_per_sm > 0) bps = std::min(bps, h->blocks_per_sm);
+      if (bps <= 0)
+        return fail(h, MTP_E_CAPACITY, "the evaluation block does not fit in shared memory for this basis and max_nbr");
+      c = mtp_handle::LaunchChoice{h->threads, bps, true, 0, 1};
     }
-  }
-  if (bps <= 0) {
-    lanes = h->threads;
-    int st = get_schedule(h, lanes, &ds);
+    DeviceSchedule* ds = nullptr;
+    int st = get_schedule(h, c.lanes, &ds);
     if (st != MTP_OK) return st;
-    vglobal = true;
-    bps = eval_blocks_per_sm(make_model(h, *ds), stride, lanes, fp64, true);
+    c.smem = eval_smem_bytes(make_model(h, *ds), stride, c.lanes, fp64, c.vglobal, c.A);
+    h->launch_cache[key] = c;
   }
-  if (bps <= 0)
-    return fail(h, MTP_E_CAPACITY, "the evaluation block does not fit in shared memory for this basis and max_nbr");
-  if (h->blocks_per_sm > 0) bps = std::min(bps, h->blocks_per_sm);
-  long long blocks = static_cast<long long>(bps) * h->sm_count;
-  blocks = std::max(1LL, std::min<long long>(blocks, natoms));
-  if (vglobal) {
-    const size_t need = static_cast<size_t>(blocks) * ds->sched.v_size * (fp64 ? sizeof(double) : sizeof(float));
+  DeviceSchedule* ds = nullptr;
+  int st = get_schedule(h, c.lanes, &ds);
+  if (st != MTP_OK) return st;
+  const long long groups = (static_cast<long long>(natoms) + c.A - 1) / c.A;
+  const long long blocks = std::max(1LL, std::min<long long>(static_cast<long long>(c.bps) * h->sm_count, groups));
+  if (c.vglobal) {
+    const size_t need = static_cast<size_t>(blocks) * ds->sched.v_size * c.A * (fp64 ? sizeof(double) : sizeof(float));
     if (need > h->vscratch_bytes) {
       if (h->d_vscratch) cudaFree(h->d_vscratch);
       h->d_vscratch = nullptr;
@@ -279,13 +283,13 @@ int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, 
   }
   *ds_out = ds;
   *blocks_out = static_cast<int>(blocks);
-  *vglobal_out = vglobal;
-  h->last_threads = lanes;
+  *vglobal_out = c.vglobal;
+  h->last_threads = c.lanes;
   h->last_blocks = static_cast<int>(blocks);
-  h->last_bps = bps;
-  h->last_vglobal = vglobal;
-  h->last_smem = eval_smem_bytes(make_model(h, *ds), stride, lanes, fp64, vglobal);
-  h->launch_cache[key] = mtp_handle::LaunchChoice{lanes, bps, vglobal, h->last_smem};
+  h->last_bps = c.bps;
+  h->last_vglobal = c.vglobal;
+  h->last_smem = c.smem;
+  h->last_apb = c.A;
   return MTP_OK;
 }
 
@@ -328,7 +332,7 @@ int run_device(mtp_handle* h, int natoms, int stride, const int* itypes, const d
     ++h->prof_used;
     MTP_CUDA(h, cudaEventRecord(e0, h->stream));
   }
-  MTP_CUDA(h, launch_eval(md, io, h->last_threads, blocks, fp64, vglobal, h->stream));
+  MTP_CUDA(h, launch_eval(md, io, h->last_threads, blocks, fp64, vglobal, h->last_apb, h->stream));
   if (e1) MTP_CUDA(h, cudaEventRecord(e1, h->stream));
   MTP_CUDA(h, launch_force_gather(natoms, stride, rijs, counts, h->d_G, h->d_in_ptr, h->d_in_slot, forces,
                                   h->d_wown, vatom, h->stream));
@@ -521,21 +525,25 @@ int mtp_set_coeffs(mtp_handle* h, const double* species, const double* moment, c
   return upload_coeffs(h);
 }
 
-int mtp_set_launch(mtp_handle* h, int threads, int bps) {
+int mtp_set_launch(mtp_handle* h, int threads, int bps, int apb) {
   if (!h) return MTP_E_INVALID;
-  if (threads != 64 && threads != 128 && threads != 256 && threads != 512)
-    return fail(h, MTP_E_INVALID, "threads_per_block must be 64, 128, 256 or 512");
+  if (threads != 128 && threads != 256 && threads != 512)
+    return fail(h, MTP_E_INVALID, "threads_per_block must be 128, 256 or 512");
+  if (apb != 0 && apb != 1 && apb != 2 && apb != 4)
+    return fail(h, MTP_E_INVALID, "atoms_per_block must be 0 (automatic), 1, 2 or 4");
   h->threads = threads;
   h->blocks_per_sm = std::max(0, bps);
+  h->apb = apb;
   return MTP_OK;
 }
 
-int mtp_get_launch(const mtp_handle* h, int* out4) {
-  if (!h || !out4) return MTP_E_INVALID;
-  out4[0] = h->last_threads;
-  out4[1] = h->last_blocks;
-  out4[2] = static_cast<int>(h->last_smem);
-  out4[3] = h->last_bps;
+int mtp_get_launch(const mtp_handle* h, int* out5) {
+  if (!h || !out5) return MTP_E_INVALID;
+  out5[0] = h->last_threads;
+  out5[1] = h->last_blocks;
+  out5[2] = static_cast<int>(h->last_smem);
+  out5[3] = h->last_bps;
+  out5[4] = h->last_apb;
   return MTP_OK;
 }
 

@@ -75,39 +75,41 @@ struct DevIO {
 };
 
 // Shared-memory carve of the evaluation kernel.
-// Depth of the per-thread prefetch ring of lane-program entries.
-constexpr int kRing = 8;
+// Lane-program entries requested ahead of use (registers), per thread.
+constexpr int kPrefetch = 8;
 
+// Shared-memory carve of the evaluation kernel for A atoms per block: the
+// value space is interleaved [slot][atom] so one vector access serves all A
+// atoms; neighbour staging is kept per atom.
 struct SmemLayout {
   int pws;        // stride of a power row (3 (D+1), rounded up to odd)
-  size_t v, rad, u, f, fp, pw, slot, abc, mk, red, cnt, ring, total;
+  size_t v, rad, u, f, fp, pw, slot, abc, mk, red, cnt, total;
 };
 
 template <typename T>
 __host__ __device__ inline SmemLayout smem_layout(int v_size, int S, int R, int K, int P, int D, int n_pad,
-                                                  int threads) {
+                                                  int threads, int A) {
   SmemLayout L;
   L.pws = 3 * (D + 1);
   if ((L.pws & 1) == 0) L.pws += 1;
   size_t o = 0;
   auto take = [&](size_t bytes) {
-    size_t at = (o + 15) & ~size_t(15);
+    size_t at = (o + 31) & ~size_t(31);
     o = at + bytes;
     return at;
   };
-  L.v = take(sizeof(T) * v_size);
+  L.v = take(sizeof(T) * v_size * A);
   L.rad = take(sizeof(T) * S * S * R * K);
-  L.u = take(sizeof(T) * 4 * n_pad);
-  L.f = take(sizeof(T) * R * n_pad);
-  L.fp = take(sizeof(T) * R * n_pad);
-  L.pw = take(sizeof(T) * L.pws * n_pad);
-  L.slot = take(sizeof(int) * n_pad);
+  L.u = take(sizeof(T) * 4 * n_pad * A);
+  L.f = take(sizeof(T) * R * n_pad * A);
+  L.fp = take(sizeof(T) * R * n_pad * A);
+  L.pw = take(sizeof(T) * L.pws * n_pad * A);
+  L.slot = take(sizeof(int) * n_pad * A);
   L.abc = take(sizeof(int) * 4 * P);
   L.mk = take(sizeof(int) * kMaxR * P);
-  L.red = take(sizeof(double) * (threads / 32));
+  L.red = take(sizeof(double) * (threads / 32) * A);
   L.cnt = take(sizeof(int) * (threads / 32 + 1));
-  L.ring = take(sizeof(uint2) * kRing * threads);
-  L.total = (o + 15) & ~size_t(15);
+  L.total = (o + 31) & ~size_t(31);
   return L;
 }
 
@@ -116,299 +118,349 @@ __device__ __forceinline__ float dev_sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double dev_fma(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float dev_fma(float a, float b, float c) { return fmaf(a, b, c); }
 
-// Asynchronous 8-byte global -> shared copy (cp.async, cached in L1).
-__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// Stream one lane program pass through a per-thread ring of kRing entries in
-// shared memory: entry e lives in ring slot e % kRing and is requested
-// kRing - 1 steps before it is used, so the L2 latency of the program (the
-// whole schedule is ~1 MB at level 24 and cannot stay in L1) overlaps the
-// arithmetic of the preceding steps.  The ring column of a thread is written
-// and read by that thread only.
-template <typename Body>
-__device__ __forceinline__ void stream_pass(const uint2* __restrict__ ent, int steps, int lanes, int tid,
-                                            uint2* __restrict__ ring, Body& body) {
-  const uint2* p = ent + tid;
-#pragma unroll
-  for (int k = 0; k < kRing; ++k) {
-    if (k < steps) cp_async8(ring + k * lanes + tid, p + static_cast<size_t>(k) * lanes);
-    cp_async_commit();
-  }
-  for (int s = 0; s < steps; ++s) {
-    if (s >= 1) {
-      const int nx = s + kRing - 1;   // refills the slot read in the previous step
-      if (nx < steps) cp_async8(ring + (nx % kRing) * lanes + tid, p + static_cast<size_t>(nx) * lanes);
-      cp_async_commit();
-    }
-    cp_async_wait<kRing - 1>();
-    const uint2 e = ring[(s % kRing) * lanes + tid];
-    body(e);
-  }
-  cp_async_wait<0>();
-}
-
-// acc += c * V[a] * V[b]; on STORE/ADD write the accumulator and restart.
-template <typename T>
-struct PlainBody {
-  T* V;
-  T acc;
-  __device__ __forceinline__ void operator()(const uint2 e) {
-    const T c = static_cast<T>(e.y >> 18);
-    acc = dev_fma(c * V[e.x & 0xFFFFu], V[e.x >> 16], acc);
-    const uint32_t op = (e.y >> 16) & 3u;
-    if (op) {
-      const uint32_t d = e.y & 0xFFFFu;
-      if (op == kOpStore) V[d] = acc;
-      else V[d] += acc;
-      acc = T(0);
-    }
-  }
+// A values of one value-space slot, loaded/stored as one vector access.
+template <typename T, int A>
+struct __align__(sizeof(T) * A) Pack {
+  T v[A];
 };
 
-// Execute one lane program pass with the plain arithmetic.
-template <typename T>
+// Stream one lane program pass: every thread walks its column of the
+// [steps][lanes] entry array with kPrefetch entries in flight (registers), so
+// the L2 latency of the program overlaps the arithmetic.  Each entry feeds A
+// atoms: acc[a] += c * V[x][a] * V[y][a]; STORE/ADD flush into V[d][a].
+template <typename T, int A>
 __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int steps, int lanes, int tid,
-                                         T* __restrict__ V, uint2* __restrict__ ring) {
-  PlainBody<T> body{V, T(0)};
-  stream_pass(ent, steps, lanes, tid, ring, body);
+                                         T* __restrict__ V) {
+  const uint2* p = ent + tid;
+  uint2 buf[kPrefetch];
+#pragma unroll
+  for (int k = 0; k < kPrefetch; ++k) buf[k] = k < steps ? __ldg(p + static_cast<size_t>(k) * lanes) : make_uint2(0u, 0u);
+  T acc[A];
+#pragma unroll
+  for (int a = 0; a < A; ++a) acc[a] = T(0);
+  for (int s0 = 0; s0 < steps; s0 += kPrefetch) {
+#pragma unroll
+    for (int k = 0; k < kPrefetch; ++k) {
+      if (s0 + k < steps) {
+        const uint2 e = buf[k];
+        const int nx = s0 + k + kPrefetch;
+        if (nx < steps) buf[k] = __ldg(p + static_cast<size_t>(nx) * lanes);
+        const T c = static_cast<T>(e.y >> 18);
+        const Pack<T, A> va = *reinterpret_cast<const Pack<T, A>*>(V + (e.x & 0xFFFFu) * A);
+        const Pack<T, A> vb = *reinterpret_cast<const Pack<T, A>*>(V + (e.x >> 16) * A);
+#pragma unroll
+        for (int a = 0; a < A; ++a) acc[a] = dev_fma(c * va.v[a], vb.v[a], acc[a]);
+        const uint32_t op = (e.y >> 16) & 3u;
+        if (op) {
+          Pack<T, A>* dst = reinterpret_cast<Pack<T, A>*>(V + (e.y & 0xFFFFu) * A);
+          Pack<T, A> out;
+          if (op == kOpStore) {
+#pragma unroll
+            for (int a = 0; a < A; ++a) out.v[a] = acc[a];
+          } else {
+            out = *dst;
+#pragma unroll
+            for (int a = 0; a < A; ++a) out.v[a] += acc[a];
+          }
+          *dst = out;
+#pragma unroll
+          for (int a = 0; a < A; ++a) acc[a] = T(0);
+        }
+      }
+    }
+  }
 }
 
-// Deterministic block sum of one double per thread (valid in thread 0).
-__device__ __forceinline__ double block_sum(double v, double* red) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  double s = 0.0;
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < static_cast<int>(blockDim.x >> 5); ++i) s += red[i];
+// Generic lane-program streamer (used by the dual-number kernels): every thread
+// walks its column of the [steps][lanes] entries with kPrefetch in flight.
+template <typename Body>
+__device__ __forceinline__ void stream_entries(const uint2* __restrict__ ent, int steps, int lanes, int tid,
+                                               Body& body) {
+  const uint2* p = ent + tid;
+  uint2 buf[kPrefetch];
+#pragma unroll
+  for (int k = 0; k < kPrefetch; ++k) buf[k] = k < steps ? __ldg(p + static_cast<size_t>(k) * lanes) : make_uint2(0u, 0u);
+  for (int s0 = 0; s0 < steps; s0 += kPrefetch) {
+#pragma unroll
+    for (int k = 0; k < kPrefetch; ++k) {
+      if (s0 + k < steps) {
+        const uint2 e = buf[k];
+        const int nx = s0 + k + kPrefetch;
+        if (nx < steps) buf[k] = __ldg(p + static_cast<size_t>(nx) * lanes);
+        body(e);
+      }
+    }
+  }
+}
+
+// Deterministic block sums of A doubles per thread (valid in thread 0).
+template <int A>
+__device__ __forceinline__ void block_sum(double (&v)[A], double* red) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int a = 0; a < A; ++a) {
+    for (int o = 16; o > 0; o >>= 1) v[a] += __shfl_xor_sync(0xffffffffu, v[a], o);
+    if (l == 0) red[a * nw + w] = v[a];
   }
   __syncthreads();
-  return s;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int a = 0; a < A; ++a) {
+      double s = 0.0;
+      for (int i = 0; i < nw; ++i) s += red[a * nw + i];
+      v[a] = s;
+    }
+  }
+  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
 // evaluation kernel
 // ---------------------------------------------------------------------------
-// kVGlobal: the per-atom value space (moments, adjoints, partials) is a
-// private slice of global memory (L1/L2-resident) instead of shared memory;
-// used when it does not fit in shared memory (level 28 in FP64).
-template <typename T, bool kVGlobal>
+// A atoms per block share every lane-program entry.  kVGlobal: the value
+// space (moments, adjoints, partials) is a private slice of global memory
+// (L1/L2-resident) instead of shared memory; used when it does not fit in
+// shared memory (level 28 in FP64).
+template <typename T, bool kVGlobal, int A>
 __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(32) unsigned char smem[];
   const int NT = blockDim.x;
   const int tid = threadIdx.x;
-  const SmemLayout L = smem_layout<T>(kVGlobal ? 0 : md.v_size, md.S, md.R, md.K, md.P, md.D, io.n_pad, NT);
-  T* V = kVGlobal ? reinterpret_cast<T*>(io.vscratch) + static_cast<size_t>(blockIdx.x) * md.v_size
+  const SmemLayout L = smem_layout<T>(kVGlobal ? 0 : md.v_size, md.S, md.R, md.K, md.P, md.D, io.n_pad, NT, A);
+  T* V = kVGlobal ? reinterpret_cast<T*>(io.vscratch) + static_cast<size_t>(blockIdx.x) * md.v_size * A
                   : reinterpret_cast<T*>(smem + L.v);
   T* sRad = reinterpret_cast<T*>(smem + L.rad);
-  T* sU = reinterpret_cast<T*>(smem + L.u);
-  T* sF = reinterpret_cast<T*>(smem + L.f);
-  T* sFp = reinterpret_cast<T*>(smem + L.fp);
-  T* sPw = reinterpret_cast<T*>(smem + L.pw);
-  int* sSlot = reinterpret_cast<int*>(smem + L.slot);
   int* sAbc = reinterpret_cast<int*>(smem + L.abc);
   int* sMk = reinterpret_cast<int*>(smem + L.mk);
   double* sRed = reinterpret_cast<double*>(smem + L.red);
   int* sCnt = reinterpret_cast<int*>(smem + L.cnt);
-  uint2* sRing = reinterpret_cast<uint2*>(smem + L.ring);
+  const int n_pad = io.n_pad;
 
   const int S = md.S, R = md.R, K = md.K, P = md.P, D1 = md.D + 1, pws = L.pws;
   // per-block constants
   for (int x = tid; x < S * S * R * K; x += NT) sRad[x] = static_cast<T>(md.radial[x]);
   for (int x = tid; x < 4 * P; x += NT) sAbc[x] = md.mono_abc[x];
   for (int x = tid; x < kMaxR * P; x += NT) sMk[x] = md.mono_k[x];
-  for (int x = tid; x < md.nzero; x += NT) V[md.v_m + md.zero_list[x]] = T(0);
-  if (tid == 0) {
-    V[md.v_zero] = T(0);
-    V[md.v_one] = T(1);
+  for (int x = tid; x < md.nzero * A; x += NT) V[(md.v_m + md.zero_list[x / A]) * A + x % A] = T(0);
+  for (int a = tid; a < A; a += NT) {
+    V[md.v_zero * A + a] = T(0);
+    V[md.v_one * A + a] = T(1);
   }
-  const T rmin = static_cast<T>(md.rmin), rmax = static_cast<T>(md.rmax);
+  const T rmax = static_cast<T>(md.rmax);
   const T inv_range = static_cast<T>(1.0 / (md.rmax - md.rmin));
   const T rsum = static_cast<T>(md.rmin + md.rmax);
   const T scal = static_cast<T>(md.scaling);
   __syncthreads();
 
-  for (int atom = blockIdx.x; atom < io.natoms; atom += gridDim.x) {
-    int it = __ldg(io.itypes + atom);
-    if (it < 0 || it >= S) {
-      if (tid == 0) atomicOr(io.err, kErrSpecies);
-      it = 0;
-    }
-    int cnt = io.counts ? __ldg(io.counts + atom) : io.nbr_stride;
-    if (cnt > io.n_pad || cnt < 0) {
-      if (tid == 0) atomicOr(io.err, kErrCapacity);
-      cnt = cnt < 0 ? 0 : io.n_pad;
-    }
-    const double* rrow = io.rijs + static_cast<size_t>(atom) * io.nbr_stride * 3;
-    const int* trow = io.jtypes + static_cast<size_t>(atom) * io.nbr_stride;
-    double* grow = io.pair_grad + static_cast<size_t>(atom) * io.nbr_stride * 3;
-
-    // ---- N1: stage the valid neighbours ---------------------------------
-    int nv = 0;
-    for (int s0 = 0; s0 < io.nbr_stride; s0 += NT) {
-      const int s = s0 + tid;
-      bool valid = false;
-      T rx = T(0), ry = T(0), rz = T(0), d = T(0);
-      int jt = -1;
-      if (s < io.nbr_stride) {
-        if (s < cnt) {
-          jt = __ldg(trow + s);
-          rx = static_cast<T>(__ldg(rrow + 3 * s));
-          ry = static_cast<T>(__ldg(rrow + 3 * s + 1));
-          rz = static_cast<T>(__ldg(rrow + 3 * s + 2));
-          if (jt >= S) {
-            atomicOr(io.err, kErrSpecies);
-            jt = -1;
-          }
-          const T r2 = rx * rx + ry * ry + rz * rz;
-          d = dev_sqrt(r2);
-          valid = (jt >= 0) && (r2 > T(0)) && (d < rmax);
-        }
-        if (!valid) {
-          grow[3 * s] = 0.0;
-          grow[3 * s + 1] = 0.0;
-          grow[3 * s + 2] = 0.0;
-        }
-      }
-      const unsigned bal = __ballot_sync(0xffffffffu, valid);
-      const int w = tid >> 5, l = tid & 31;
-      if (l == 0) sCnt[w] = __popc(bal);
-      __syncthreads();
-      if (tid == 0) {
-        int acc = 0;
-        for (int i = 0; i < (NT >> 5); ++i) {
-          int c = sCnt[i];
-          sCnt[i] = acc;
-          acc += c;
-        }
-        sCnt[NT >> 5] = acc;
-      }
-      __syncthreads();
-      if (valid) {
-        const int q = nv + sCnt[w] + __popc(bal & ((1u << l) - 1u));
-        const T inv_d = T(1) / d;
-        const T ux = rx * inv_d, uy = ry * inv_d, uz = rz * inv_d;
-        sU[4 * q] = ux;
-        sU[4 * q + 1] = uy;
-        sU[4 * q + 2] = uz;
-        sU[4 * q + 3] = d;
-        sSlot[q] = s;
-        // Chebyshev T_n(x) and dT_n/dx by their recurrences, folded into
-        // sum_n c[t_i, t_j, mu, n] T_n for every mu as the terms appear
-        const T x = (T(2) * d - rsum) * inv_range;
-        const T dxdd = T(2) * inv_range;
-        const T* c = sRad + (static_cast<size_t>(it) * S + jt) * R * K;
-        T base[kMaxR], dbase[kMaxR];
+  for (int base = blockIdx.x * A; base < io.natoms; base += gridDim.x * A) {
+    int it_a[A], nv_a[A];
+    // ---- N1 + N2 per atom of the group -------------------------------------
 #pragma unroll
-        for (int mu = 0; mu < kMaxR; ++mu) {
-          base[mu] = mu < R ? c[mu * K] : T(0);   // T_0 = 1, T_0' = 0
-          dbase[mu] = T(0);
+    for (int a = 0; a < A; ++a) {
+      const int atom = base + a;
+      const bool real = atom < io.natoms;
+      int it = real ? __ldg(io.itypes + atom) : 0;
+      if (it < 0 || it >= S) {
+        if (tid == 0) atomicOr(io.err, kErrSpecies);
+        it = 0;
+      }
+      it_a[a] = it;
+      int cnt = real ? (io.counts ? __ldg(io.counts + atom) : io.nbr_stride) : 0;
+      if (cnt > n_pad || cnt < 0) {
+        if (tid == 0) atomicOr(io.err, kErrCapacity);
+        cnt = cnt < 0 ? 0 : n_pad;
+      }
+      const size_t arow = static_cast<size_t>(real ? atom : 0) * io.nbr_stride;
+      const double* rrow = io.rijs + arow * 3;
+      const int* trow = io.jtypes + arow;
+      double* grow = io.pair_grad + arow * 3;
+      T* sU = reinterpret_cast<T*>(smem + L.u) + static_cast<size_t>(a) * 4 * n_pad;
+      T* sF = reinterpret_cast<T*>(smem + L.f) + static_cast<size_t>(a) * R * n_pad;
+      T* sFp = reinterpret_cast<T*>(smem + L.fp) + static_cast<size_t>(a) * R * n_pad;
+      T* sPw = reinterpret_cast<T*>(smem + L.pw) + static_cast<size_t>(a) * pws * n_pad;
+      int* sSlot = reinterpret_cast<int*>(smem + L.slot) + a * n_pad;
+
+      int nv = 0;
+      for (int s0 = 0; s0 < io.nbr_stride; s0 += NT) {
+        const int s = s0 + tid;
+        bool valid = false;
+        T rx = T(0), ry = T(0), rz = T(0), d = T(0);
+        int jt = -1;
+        if (real && s < io.nbr_stride) {
+          if (s < cnt) {
+            jt = __ldg(trow + s);
+            rx = static_cast<T>(__ldg(rrow + 3 * s));
+            ry = static_cast<T>(__ldg(rrow + 3 * s + 1));
+            rz = static_cast<T>(__ldg(rrow + 3 * s + 2));
+            if (jt >= S) {
+              atomicOr(io.err, kErrSpecies);
+              jt = -1;
+            }
+            const T r2 = rx * rx + ry * ry + rz * rz;
+            d = dev_sqrt(r2);
+            valid = (jt >= 0) && (r2 > T(0)) && (d < rmax);
+          }
+          if (!valid) {
+            grow[3 * s] = 0.0;
+            grow[3 * s + 1] = 0.0;
+            grow[3 * s + 2] = 0.0;
+          }
         }
-        T t_prev = T(1), t_cur = x, dt_prev = T(0), dt_cur = T(1);
-        for (int n = 1; n < K; ++n) {
+        const unsigned bal = __ballot_sync(0xffffffffu, valid);
+        const int w = tid >> 5, l = tid & 31;
+        if (l == 0) sCnt[w] = __popc(bal);
+        __syncthreads();
+        if (tid == 0) {
+          int accn = 0;
+          for (int i = 0; i < (NT >> 5); ++i) {
+            int c = sCnt[i];
+            sCnt[i] = accn;
+            accn += c;
+          }
+          sCnt[NT >> 5] = accn;
+        }
+        __syncthreads();
+        if (valid) {
+          const int q = nv + sCnt[w] + __popc(bal & ((1u << l) - 1u));
+          const T inv_d = T(1) / d;
+          const T ux = rx * inv_d, uy = ry * inv_d, uz = rz * inv_d;
+          sU[4 * q] = ux;
+          sU[4 * q + 1] = uy;
+          sU[4 * q + 2] = uz;
+          sU[4 * q + 3] = d;
+          sSlot[q] = s;
+          // Chebyshev T_n(x) and dT_n/dx by their recurrences, folded into
+          // sum_n c[t_i, t_j, mu, n] T_n for every mu as the terms appear
+          const T x = (T(2) * d - rsum) * inv_range;
+          const T dxdd = T(2) * inv_range;
+          const T* c = sRad + (static_cast<size_t>(it) * S + jt) * R * K;
+          T bas[kMaxR], dbas[kMaxR];
+#pragma unroll
+          for (int mu = 0; mu < kMaxR; ++mu) {
+            bas[mu] = mu < R ? c[mu * K] : T(0);   // T_0 = 1, T_0' = 0
+            dbas[mu] = T(0);
+          }
+          T t_prev = T(1), t_cur = x, dt_prev = T(0), dt_cur = T(1);
+          for (int n = 1; n < K; ++n) {
+#pragma unroll
+            for (int mu = 0; mu < kMaxR; ++mu) {
+              if (mu < R) {
+                bas[mu] = dev_fma(c[mu * K + n], t_cur, bas[mu]);
+                dbas[mu] = dev_fma(c[mu * K + n], dt_cur, dbas[mu]);
+              }
+            }
+            const T t_next = T(2) * x * t_cur - t_prev;
+            const T dt_next = T(2) * t_cur + T(2) * x * dt_cur - dt_prev;
+            t_prev = t_cur;
+            t_cur = t_next;
+            dt_prev = dt_cur;
+            dt_cur = dt_next;
+          }
+          const T gap = rmax - d;
+          const T smooth = gap * gap;
 #pragma unroll
           for (int mu = 0; mu < kMaxR; ++mu) {
             if (mu < R) {
-              base[mu] = dev_fma(c[mu * K + n], t_cur, base[mu]);
-              dbase[mu] = dev_fma(c[mu * K + n], dt_cur, dbase[mu]);
+              sF[q * R + mu] = scal * smooth * bas[mu];
+              sFp[q * R + mu] = scal * (T(-2) * gap * bas[mu] + smooth * dbas[mu] * dxdd);
             }
           }
-          const T t_next = T(2) * x * t_cur - t_prev;
-          const T dt_next = T(2) * t_cur + T(2) * x * dt_cur - dt_prev;
-          t_prev = t_cur;
-          t_cur = t_next;
-          dt_prev = dt_cur;
-          dt_cur = dt_next;
+          T* pw = sPw + q * pws;
+          T px = T(1), py = T(1), pz = T(1);
+          for (int e = 0; e < D1; ++e) {
+            pw[e] = px;
+            pw[D1 + e] = py;
+            pw[2 * D1 + e] = pz;
+            px *= ux;
+            py *= uy;
+            pz *= uz;
+          }
         }
-        const T gap = rmax - d;
-        const T smooth = gap * gap;
+        nv += sCnt[NT >> 5];
+        __syncthreads();
+      }
+      nv_a[a] = nv;
+
+      // basic moments m[(mu, a, b, c)] of this atom into value lane a
+      for (int p = tid; p < P; p += NT) {
+        const int ea = sAbc[4 * p], eb = sAbc[4 * p + 1], ec = sAbc[4 * p + 2];
+        T acc[kMaxR];
+#pragma unroll
+        for (int mu = 0; mu < kMaxR; ++mu) acc[mu] = T(0);
+        for (int q = 0; q < nv; ++q) {
+          const T* pw = sPw + q * pws;
+          const T mono = pw[ea] * pw[D1 + eb] * pw[2 * D1 + ec];
+          const T* f = sF + q * R;
+#pragma unroll
+          for (int mu = 0; mu < kMaxR; ++mu)
+            if (mu < R) acc[mu] = dev_fma(f[mu], mono, acc[mu]);
+        }
 #pragma unroll
         for (int mu = 0; mu < kMaxR; ++mu) {
           if (mu < R) {
-            sF[q * R + mu] = scal * smooth * base[mu];
-            sFp[q * R + mu] = scal * (T(-2) * gap * base[mu] + smooth * dbase[mu] * dxdd);
+            const int k = sMk[kMaxR * p + mu];
+            if (k >= 0) V[(md.v_m + k) * A + a] = acc[mu];
           }
-        }
-        T* pw = sPw + q * pws;
-        T px = T(1), py = T(1), pz = T(1);
-        for (int e = 0; e < D1; ++e) {
-          pw[e] = px;
-          pw[D1 + e] = py;
-          pw[2 * D1 + e] = pz;
-          px *= ux;
-          py *= uy;
-          pz *= uz;
-        }
-      }
-      nv += sCnt[NT >> 5];
-      __syncthreads();
-    }
-
-    // ---- N2: basic moments ----------------------------------------------
-    for (int p = tid; p < P; p += NT) {
-      const int a = sAbc[4 * p], b = sAbc[4 * p + 1], cc = sAbc[4 * p + 2];
-      T acc[kMaxR];
-#pragma unroll
-      for (int mu = 0; mu < kMaxR; ++mu) acc[mu] = T(0);
-      for (int q = 0; q < nv; ++q) {
-        const T* pw = sPw + q * pws;
-        const T mono = pw[a] * pw[D1 + b] * pw[2 * D1 + cc];
-        const T* f = sF + q * R;
-#pragma unroll
-        for (int mu = 0; mu < kMaxR; ++mu)
-          if (mu < R) acc[mu] = dev_fma(f[mu], mono, acc[mu]);
-      }
-#pragma unroll
-      for (int mu = 0; mu < kMaxR; ++mu) {
-        if (mu < R) {
-          const int k = sMk[kMaxR * p + mu];
-          if (k >= 0) V[md.v_m + k] = acc[mu];
         }
       }
     }
     // adjoint seeds
-    for (int x = tid; x < md.M; x += NT) V[md.v_dm + x] = T(0);
+    for (int x = tid; x < md.M * A; x += NT) V[md.v_dm * A + x] = T(0);
     __syncthreads();
-    for (int x = tid; x < md.nseed; x += NT) V[md.v_dm + md.seed_idx[x]] = static_cast<T>(md.seed_val[x]);
+    for (int x = tid; x < md.nseed * A; x += NT)
+      V[(md.v_dm + md.seed_idx[x / A]) * A + x % A] = static_cast<T>(md.seed_val[x / A]);
 
     // ---- T: forward contraction passes ----------------------------------
     for (int ps = 0; ps < md.nfwd; ++ps) {
-      run_pass<T>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, V, sRing);
+      run_pass<T, A>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, V);
       __syncthreads();
     }
     // energy: E_i = xi[t_i] + sum_alpha theta_alpha m[map_alpha] in FP64
-    double epart = 0.0;
-    for (int a = tid; a < md.Sa; a += NT)
-      epart = fma(__ldg(md.theta + a), static_cast<double>(V[md.v_m + __ldg(md.mapping + a)]), epart);
-    const double esum = block_sum(epart, sRed);
-    if (tid == 0) {
-      const double e = __ldg(md.species + it) + esum;
-      io.site_energy[atom] = e;
-      if (!isfinite(e)) atomicOr(io.err, kErrNonFinite);
+    {
+      double ep[A];
+#pragma unroll
+      for (int a = 0; a < A; ++a) ep[a] = 0.0;
+      for (int al = tid; al < md.Sa; al += NT) {
+        const double th = __ldg(md.theta + al);
+        const int k = md.v_m + __ldg(md.mapping + al);
+#pragma unroll
+        for (int a = 0; a < A; ++a) ep[a] = fma(th, static_cast<double>(V[k * A + a]), ep[a]);
+      }
+      block_sum<A>(ep, sRed);
+      if (tid == 0) {
+#pragma unroll
+        for (int a = 0; a < A; ++a) {
+          if (base + a < io.natoms) {
+            const double e = __ldg(md.species + it_a[a]) + ep[a];
+            io.site_energy[base + a] = e;
+            if (!isfinite(e)) atomicOr(io.err, kErrNonFinite);
+          }
+        }
+      }
     }
 
     // ---- R: reverse passes (dE/dm) ---------------------------------------
     for (int ps = 0; ps < md.nrev; ++ps) {
-      run_pass<T>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, V, sRing);
+      run_pass<T, A>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, V);
       __syncthreads();
     }
 
     // ---- N3: dE_i/dr_ij per kept neighbour -------------------------------
-    {
+#pragma unroll
+    for (int a = 0; a < A; ++a) {
+      const int atom = base + a;
+      const int nv = nv_a[a];
+      const T* sU = reinterpret_cast<T*>(smem + L.u) + static_cast<size_t>(a) * 4 * n_pad;
+      const T* sF = reinterpret_cast<T*>(smem + L.f) + static_cast<size_t>(a) * R * n_pad;
+      const T* sFp = reinterpret_cast<T*>(smem + L.fp) + static_cast<size_t>(a) * R * n_pad;
+      const T* sPw = reinterpret_cast<T*>(smem + L.pw) + static_cast<size_t>(a) * pws * n_pad;
+      const int* sSlot = reinterpret_cast<int*>(smem + L.slot) + a * n_pad;
+      double* grow = io.pair_grad + static_cast<size_t>(atom < io.natoms ? atom : 0) * io.nbr_stride * 3;
       int tpn = 32;
       while (tpn > 1 && tpn * nv > NT) tpn >>= 1;
       const int total = nv * tpn;
-      for (int base = 0; base < total; base += NT) {
-        const int idx = base + tid;
+      for (int b0 = 0; b0 < total; b0 += NT) {
+        const int idx = b0 + tid;
         const bool active = idx < total;
         const int q = active ? idx / tpn : 0;
         const int sl = idx & (tpn - 1);
@@ -422,25 +474,24 @@ __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
           }
           const T* pw = sPw + q * pws;
           for (int p = sl; p < P; p += tpn) {
-            const int a = sAbc[4 * p], b = sAbc[4 * p + 1], cc = sAbc[4 * p + 2];
+            const int ea = sAbc[4 * p], eb = sAbc[4 * p + 1], ec = sAbc[4 * p + 2];
             T W = T(0), Wp = T(0);
 #pragma unroll
             for (int mu = 0; mu < kMaxR; ++mu) {
               if (mu < R) {
                 const int k = sMk[kMaxR * p + mu];
                 if (k >= 0) {
-                  const T g = V[md.v_dm + k];
+                  const T g = V[(md.v_dm + k) * A + a];
                   W = dev_fma(g, f[mu], W);
                   Wp = dev_fma(g, fp[mu], Wp);
                 }
               }
             }
-            const T px = pw[a], py = pw[D1 + b], pz = pw[2 * D1 + cc];
+            const T px = pw[ea], py = pw[D1 + eb], pz = pw[2 * D1 + ec];
             Ssum = dev_fma(Wp, px * py * pz, Ssum);
-            const T am = static_cast<T>(a), bm = static_cast<T>(b), cm = static_cast<T>(cc);
-            Gx = dev_fma(W * am, pw[a > 0 ? a - 1 : 0] * py * pz, Gx);
-            Gy = dev_fma(W * bm, px * pw[D1 + (b > 0 ? b - 1 : 0)] * pz, Gy);
-            Gz = dev_fma(W * cm, px * py * pw[2 * D1 + (cc > 0 ? cc - 1 : 0)], Gz);
+            Gx = dev_fma(W * static_cast<T>(ea), pw[ea > 0 ? ea - 1 : 0] * py * pz, Gx);
+            Gy = dev_fma(W * static_cast<T>(eb), px * pw[D1 + (eb > 0 ? eb - 1 : 0)] * pz, Gy);
+            Gz = dev_fma(W * static_cast<T>(ec), px * py * pw[2 * D1 + (ec > 0 ? ec - 1 : 0)], Gz);
           }
         }
         for (int o = tpn >> 1; o > 0; o >>= 1) {

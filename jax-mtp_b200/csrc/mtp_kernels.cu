@@ -3,65 +3,87 @@
 #include "mtp_launch.hpp"
 #include "mtp_md.hpp"
 
+#include <type_traits>
+
 namespace mtp {
 
 // ---------------------------------------------------------------------------
 // evaluation kernel launch
 // ---------------------------------------------------------------------------
-size_t eval_smem_bytes(const DevModel& md, int n_pad, int threads, bool fp64, bool vglobal) {
+size_t eval_smem_bytes(const DevModel& md, int n_pad, int threads, bool fp64, bool vglobal, int A) {
   const int vs = vglobal ? 0 : md.v_size;
-  SmemLayout L = fp64 ? smem_layout<double>(vs, md.S, md.R, md.K, md.P, md.D, n_pad, threads)
-                      : smem_layout<float>(vs, md.S, md.R, md.K, md.P, md.D, n_pad, threads);
+  SmemLayout L = fp64 ? smem_layout<double>(vs, md.S, md.R, md.K, md.P, md.D, n_pad, threads, A)
+                      : smem_layout<float>(vs, md.S, md.R, md.K, md.P, md.D, n_pad, threads, A);
   return L.total;
 }
 
-template <typename T, bool G>
-static int occupancy(size_t bytes, int threads) {
+namespace {
+
+template <typename T, bool G, int A>
+int occupancy_t(size_t bytes, int threads) {
   int nb = 0;
   if (bytes > 227 * 1024) return 0;
-  if (cudaFuncSetAttribute(k_mtp_eval<T, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(k_mtp_eval<T, G, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(bytes)) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_mtp_eval<T, G>, threads, bytes) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_mtp_eval<T, G, A>, threads, bytes) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   return nb;
 }
 
-int eval_blocks_per_sm(const DevModel& md, int n_pad, int threads, bool fp64, bool vglobal) {
-  const size_t bytes = eval_smem_bytes(md, n_pad, threads, fp64, vglobal);
-  if (fp64) return vglobal ? occupancy<double, true>(bytes, threads) : occupancy<double, false>(bytes, threads);
-  return vglobal ? occupancy<float, true>(bytes, threads) : occupancy<float, false>(bytes, threads);
-}
-
-template <typename T, bool G>
-static cudaError_t launch_eval_t(const DevModel& md, const DevIO& io, int threads, int blocks, size_t bytes,
-                                 cudaStream_t st) {
+template <typename T, bool G, int A>
+cudaError_t launch_t(const DevModel& md, const DevIO& io, int threads, int blocks, size_t bytes, cudaStream_t st) {
   // raise the dynamic shared-memory limit only when a larger size is needed,
   // so steady-state launches make no attribute calls (CUDA-graph capture)
   static size_t granted = 0;
   if (bytes > granted) {
-    cudaError_t e = cudaFuncSetAttribute(k_mtp_eval<T, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_mtp_eval<T, G, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(bytes));
     if (e != cudaSuccess) return e;
     granted = bytes;
   }
-  k_mtp_eval<T, G><<<blocks, threads, bytes, st>>>(md, io);
+  k_mtp_eval<T, G, A><<<blocks, threads, bytes, st>>>(md, io);
   return cudaGetLastError();
 }
 
-cudaError_t launch_eval(const DevModel& md, const DevIO& io, int threads, int blocks, bool fp64, bool vglobal,
+}  // namespace
+
+// Supported (precision, placement, atoms per block) combinations.
+#define MTP_EVAL_VARIANTS(X) \
+  X(double, false, 1) X(double, false, 2) X(double, true, 1) X(float, false, 1) X(float, false, 2) \
+  X(float, false, 4) X(float, true, 1)
+
+bool eval_variant_exists(bool fp64, bool vglobal, int A) {
+#define X(T, G, AA) \
+  if ((fp64 == std::is_same<T, double>::value) && vglobal == G && A == AA) return true;
+  MTP_EVAL_VARIANTS(X)
+#undef X
+  return false;
+}
+
+int eval_blocks_per_sm(const DevModel& md, int n_pad, int threads, bool fp64, bool vglobal, int A) {
+  const size_t bytes = eval_smem_bytes(md, n_pad, threads, fp64, vglobal, A);
+#define X(T, G, AA) \
+  if ((fp64 == std::is_same<T, double>::value) && vglobal == G && A == AA) return occupancy_t<T, G, AA>(bytes, threads);
+  MTP_EVAL_VARIANTS(X)
+#undef X
+  return 0;
+}
+
+cudaError_t launch_eval(const DevModel& md, const DevIO& io, int threads, int blocks, bool fp64, bool vglobal, int A,
                         cudaStream_t st) {
   if (io.natoms <= 0) return cudaSuccess;
-  const size_t bytes = eval_smem_bytes(md, io.n_pad, threads, fp64, vglobal);
-  if (fp64)
-    return vglobal ? launch_eval_t<double, true>(md, io, threads, blocks, bytes, st)
-                   : launch_eval_t<double, false>(md, io, threads, blocks, bytes, st);
-  return vglobal ? launch_eval_t<float, true>(md, io, threads, blocks, bytes, st)
-                 : launch_eval_t<float, false>(md, io, threads, blocks, bytes, st);
+  const size_t bytes = eval_smem_bytes(md, io.n_pad, threads, fp64, vglobal, A);
+#define X(T, G, AA) \
+  if ((fp64 == std::is_same<T, double>::value) && vglobal == G && A == AA) \
+    return launch_t<T, G, AA>(md, io, threads, blocks, bytes, st);
+  MTP_EVAL_VARIANTS(X)
+#undef X
+  return cudaErrorInvalidValue;
 }
 
 // ---------------------------------------------------------------------------

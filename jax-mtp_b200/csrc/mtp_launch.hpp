@@ -9,12 +9,14 @@ namespace mtp {
 
 constexpr int kReduceBlocks = 256;   // fixed: the reduction order never depends on the GPU
 
-// Dynamic shared memory of the evaluation kernel (vglobal: value space in
-// global memory, io.vscratch holding blocks * v_size values).
-size_t eval_smem_bytes(const DevModel& md, int n_pad, int threads, bool fp64, bool vglobal);
+// Dynamic shared memory of the evaluation kernel for A atoms per block
+// (vglobal: value space in global memory, io.vscratch holding
+// blocks * A * v_size values).
+size_t eval_smem_bytes(const DevModel& md, int n_pad, int threads, bool fp64, bool vglobal, int A);
+bool eval_variant_exists(bool fp64, bool vglobal, int A);
 // Blocks per SM that fit for the evaluation kernel (0 if it does not fit).
-int eval_blocks_per_sm(const DevModel& md, int n_pad, int threads, bool fp64, bool vglobal);
-cudaError_t launch_eval(const DevModel& md, const DevIO& io, int threads, int blocks, bool fp64, bool vglobal,
+int eval_blocks_per_sm(const DevModel& md, int n_pad, int threads, bool fp64, bool vglobal, int A);
+cudaError_t launch_eval(const DevModel& md, const DevIO& io, int threads, int blocks, bool fp64, bool vglobal, int A,
                         cudaStream_t st);
 
 // Incoming-slot lists: for every atom k, the slots (i, s) whose neighbour is k,

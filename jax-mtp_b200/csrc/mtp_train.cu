@@ -7,7 +7,7 @@ namespace mtp {
 
 struct TrainSmem {
   int pws;
-  size_t v, rad, u, du, f, fp, phi, phip, pw, A, Bv, jt, abc, mk, gth, gxi, grad, red, cnt, ring, total;
+  size_t v, rad, u, du, f, fp, phi, phip, pw, A, Bv, jt, abc, mk, gth, gxi, grad, red, cnt, total;
 };
 
 template <typename T>
@@ -41,7 +41,6 @@ __host__ __device__ inline TrainSmem train_layout(int v_size, int S, int R, int 
   L.grad = take(sizeof(double) * S * S * R * K);
   L.red = take(sizeof(double) * (threads / 32));
   L.cnt = take(sizeof(int) * (threads / 32 + 1));
-  L.ring = take(sizeof(uint2) * kRing * threads);
   L.total = (o + 15) & ~size_t(15);
   return L;
 }
@@ -106,7 +105,7 @@ struct DualRevBody {
 template <typename T, bool kVGlobal>
 __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, int n_pad, void* vscratch,
                                                      double* partials) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(32) unsigned char smem[];
   const int NT = blockDim.x, tid = threadIdx.x;
   const int S = md.S, R = md.R, K = md.K, P = md.P, D1 = md.D + 1, H = md.v_size;
   const TrainSmem L = train_layout<T>(kVGlobal ? 0 : md.v_size, S, R, K, P, md.D, md.Sa, n_pad, NT);
@@ -129,7 +128,6 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
   double* gXi = reinterpret_cast<double*>(smem + L.gxi);
   double* gRad = reinterpret_cast<double*>(smem + L.grad);
   int* sCnt = reinterpret_cast<int*>(smem + L.cnt);
-  uint2* sRing = reinterpret_cast<uint2*>(smem + L.ring);
   const int pws = L.pws;
   const int nrad = S * S * R * K;
 
@@ -353,7 +351,7 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
     // ---- dual forward tree --------------------------------------------------
     for (int ps = 0; ps < md.nfwd; ++ps) {
       DualFwdBody<T> body{V, H, T(0), T(0)};
-      stream_pass(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, sRing, body);
+      stream_entries(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, body);
       __syncthreads();
     }
     for (int a = tid; a < md.Sa; a += NT) {
@@ -365,7 +363,7 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
     // ---- dual reverse tree ---------------------------------------------------
     for (int ps = 0; ps < md.nrev; ++ps) {
       DualRevBody<T> body{V, H, T(0), T(0)};
-      stream_pass(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, sRing, body);
+      stream_entries(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, body);
       __syncthreads();
     }
 

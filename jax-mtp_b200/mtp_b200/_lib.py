@@ -39,7 +39,7 @@ SIGNATURES = {
     "mtp_sync_status": (_I, [_P]),
     "mtp_compute_batch_device": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "mtp_adjoint_batch_device": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
-    "mtp_set_launch": (_I, [_P, _I, _I]),
+    "mtp_set_launch": (_I, [_P, _I, _I, _I]),
     "mtp_get_launch": (_I, [_P, _P]),
     "mtp_parse_info": (_I, [ctypes.c_char_p, _P, ctypes.c_char_p, _I]),
     "mtp_schedule_emulate": (_I, [ctypes.c_char_p, _I, _P, _P, _P, _P]),

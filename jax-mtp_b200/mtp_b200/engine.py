@@ -96,13 +96,14 @@ class MTPEngine:
     def use_own_stream(self) -> None:
         check(lib().mtp_use_own_stream(self._h), self._h)
 
-    def set_launch(self, threads: int, blocks_per_sm: int = 0) -> None:
-        check(lib().mtp_set_launch(self._h, int(threads), int(blocks_per_sm)), self._h)
+    def set_launch(self, threads: int, blocks_per_sm: int = 0, atoms_per_block: int = 0) -> None:
+        check(lib().mtp_set_launch(self._h, int(threads), int(blocks_per_sm), int(atoms_per_block)), self._h)
 
     def launch(self) -> Dict[str, int]:
-        out = np.zeros(4, dtype=np.int32)
+        out = np.zeros(5, dtype=np.int32)
         check(lib().mtp_get_launch(self._h, _ptr(out)), self._h)
-        return {"threads": int(out[0]), "blocks": int(out[1]), "smem": int(out[2]), "blocks_per_sm": int(out[3])}
+        return {"threads": int(out[0]), "blocks": int(out[1]), "smem": int(out[2]), "blocks_per_sm": int(out[3]),
+                "atoms_per_block": int(out[4])}
 
     def sync_status(self) -> None:
         check(lib().mtp_sync_status(self._h), self._h)

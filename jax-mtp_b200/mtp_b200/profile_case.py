@@ -31,6 +31,8 @@ def main(argv=None):
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--calls", type=int, default=3)
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--apb", type=int, default=0, help="atoms per block (0: automatic)")
+    ap.add_argument("--sweep", action="store_true", help="time every (threads, atoms per block) shape")
     a = ap.parse_args(argv)
     pot = read_mtp(a.potential)
     s = synth.config2_structure(a.reps)
@@ -38,8 +40,8 @@ def main(argv=None):
     dev = torch.device("cuda")
     N = s.natoms
     with MTPEngine(a.potential, N, a.stride, precision=a.precision) as eng:
-        if a.threads:
-            eng.set_launch(a.threads)
+        if a.threads or a.apb:
+            eng.set_launch(a.threads or 256, 0, a.apb)
         x = torch.as_tensor(s.positions, device=dev)
         t = torch.as_tensor(s.types, device=dev)
         js = torch.empty((N, a.stride), dtype=torch.int32, device=dev)
@@ -48,13 +50,22 @@ def main(argv=None):
         rij = torch.empty((N, a.stride, 3), dtype=torch.float64, device=dev)
         eng.neighbors_device(x, s.cell, t, pot.max_dist + 0.3, a.stride, js, im, jt, cnt)
         eng.pack_rij_device(x, s.cell, js, im, cnt, rij)
-        eng.profile(True)
-        for k in range(a.calls):
-            eng.compute_device(t, rij, js, jt, cnt, reuse_neighbors=k > 0)
-        ms, n = eng.profile_read()
-        eng.sync_status()
-        print(json.dumps({"atoms": N, "precision": a.precision, "eval_ms_per_call": ms / max(1, n),
-                          "launch": eng.launch()}))
+        shapes = [(None, None)]
+        if a.sweep:
+            apbs = (1, 2) if a.precision == "fp64" else (1, 2, 4)
+            shapes = [(th, ap) for th in (256, 512) for ap in apbs]
+        for th, ap in shapes:
+            if th is not None:
+                eng.set_launch(th, 0, ap)
+            eng.compute_device(t, rij, js, jt, cnt)          # warm-up, builds the incoming lists
+            eng.profile(True)
+            for k in range(a.calls):
+                eng.compute_device(t, rij, js, jt, cnt, reuse_neighbors=True)
+            ms, n = eng.profile_read()
+            eng.profile(False)
+            eng.sync_status()
+            print(json.dumps({"atoms": N, "precision": a.precision, "eval_ms_per_call": ms / max(1, n),
+                              "launch": eng.launch()}), flush=True)
 
 
 if __name__ == "__main__":

@@ -19,12 +19,24 @@ size_t eval_smem_bytes(const DevModel& md, int n_pad, int threads, bool fp64, bo
 
 namespace {
 
+// The dynamic shared-memory limit of each instantiation only ever grows, so a
+// later launch never finds it lowered by an occupancy query for a smaller
+// shape, and steady-state launches make no attribute calls (graph capture).
+template <typename T, bool G, int A>
+cudaError_t ensure_smem_limit(size_t bytes) {
+  static size_t granted = 0;
+  if (bytes <= granted) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(k_mtp_eval<T, G, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(bytes));
+  if (e == cudaSuccess) granted = bytes;
+  return e;
+}
+
 template <typename T, bool G, int A>
 int occupancy_t(size_t bytes, int threads) {
   int nb = 0;
   if (bytes > 227 * 1024) return 0;
-  if (cudaFuncSetAttribute(k_mtp_eval<T, G, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(bytes)) != cudaSuccess) {
+  if (ensure_smem_limit<T, G, A>(bytes) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -37,15 +49,8 @@ int occupancy_t(size_t bytes, int threads) {
 
 template <typename T, bool G, int A>
 cudaError_t launch_t(const DevModel& md, const DevIO& io, int threads, int blocks, size_t bytes, cudaStream_t st) {
-  // raise the dynamic shared-memory limit only when a larger size is needed,
-  // so steady-state launches make no attribute calls (CUDA-graph capture)
-  static size_t granted = 0;
-  if (bytes > granted) {
-    cudaError_t e = cudaFuncSetAttribute(k_mtp_eval<T, G, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(bytes));
-    if (e != cudaSuccess) return e;
-    granted = bytes;
-  }
+  cudaError_t e = ensure_smem_limit<T, G, A>(bytes);
+  if (e != cudaSuccess) return e;
   k_mtp_eval<T, G, A><<<blocks, threads, bytes, st>>>(md, io);
   return cudaGetLastError();
 }

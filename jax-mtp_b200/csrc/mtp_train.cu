@@ -465,11 +465,20 @@ void train_free(TrainWorkspace& w) {
 }
 
 template <bool G>
+static cudaError_t adjoint_smem_limit(size_t bytes) {
+  static size_t granted = 0;
+  if (bytes <= granted) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(k_mtp_adjoint<double, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(bytes));
+  if (e == cudaSuccess) granted = bytes;
+  return e;
+}
+
+template <bool G>
 static int adjoint_occupancy(size_t bytes, int threads) {
   if (bytes > 227 * 1024) return 0;
   int nb = 0;
-  if (cudaFuncSetAttribute(k_mtp_adjoint<double, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(bytes)) != cudaSuccess) {
+  if (adjoint_smem_limit<G>(bytes) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }

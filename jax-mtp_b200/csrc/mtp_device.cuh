@@ -128,10 +128,6 @@ struct __align__(sizeof(T) * A) Pack {
 // [steps][lanes] entry array with kPrefetch entries in flight (registers), so
 // the L2 latency of the program overlaps the arithmetic.  Each entry feeds A
 // atoms: acc[a] += c * V[x][a] * V[y][a]; STORE/ADD flush into V[d][a].
-// Steps go in chunks of kPrefetch: all operand loads of a chunk are issued
-// before any of its flushes.  That is safe because no lane of a pass reads a
-// slot that any lane writes in the same pass (a property of the schedule),
-// and it lets the shared-memory latency of a whole chunk overlap.
 template <typename T, int A>
 __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int steps, int lanes, int tid,
                                          T* __restrict__ V) {
@@ -143,28 +139,20 @@ __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int step
 #pragma unroll
   for (int a = 0; a < A; ++a) acc[a] = T(0);
   for (int s0 = 0; s0 < steps; s0 += kPrefetch) {
-    uint2 e[kPrefetch];
-    Pack<T, A> va[kPrefetch], vb[kPrefetch];
-    const int n = steps - s0 < kPrefetch ? steps - s0 : kPrefetch;
 #pragma unroll
     for (int k = 0; k < kPrefetch; ++k) {
-      e[k] = buf[k];
-      if (k < n) {
+      if (s0 + k < steps) {
+        const uint2 e = buf[k];
         const int nx = s0 + k + kPrefetch;
         if (nx < steps) buf[k] = __ldg(p + static_cast<size_t>(nx) * lanes);
-        va[k] = *reinterpret_cast<const Pack<T, A>*>(V + (e[k].x & 0xFFFFu) * A);
-        vb[k] = *reinterpret_cast<const Pack<T, A>*>(V + (e[k].x >> 16) * A);
-      }
-    }
+        const T c = static_cast<T>(e.y >> 18);
+        const Pack<T, A> va = *reinterpret_cast<const Pack<T, A>*>(V + (e.x & 0xFFFFu) * A);
+        const Pack<T, A> vb = *reinterpret_cast<const Pack<T, A>*>(V + (e.x >> 16) * A);
 #pragma unroll
-    for (int k = 0; k < kPrefetch; ++k) {
-      if (k < n) {
-        const T c = static_cast<T>(e[k].y >> 18);
-#pragma unroll
-        for (int a = 0; a < A; ++a) acc[a] = dev_fma(c * va[k].v[a], vb[k].v[a], acc[a]);
-        const uint32_t op = (e[k].y >> 16) & 3u;
+        for (int a = 0; a < A; ++a) acc[a] = dev_fma(c * va.v[a], vb.v[a], acc[a]);
+        const uint32_t op = (e.y >> 16) & 3u;
         if (op) {
-          Pack<T, A>* dst = reinterpret_cast<Pack<T, A>*>(V + (e[k].y & 0xFFFFu) * A);
+          Pack<T, A>* dst = reinterpret_cast<Pack<T, A>*>(V + (e.y & 0xFFFFu) * A);
           Pack<T, A> out;
           if (op == kOpStore) {
 #pragma unroll

@@ -238,6 +238,33 @@ int mtp_verlet_device(mtp_handle* h, int natoms, double* d_x, double* d_v, const
 int mtp_profile(mtp_handle* h, int enable);
 int mtp_profile_read(mtp_handle* h, double* eval_ms, int* eval_launches);
 
+/*
+ * No counterpart in the reference.
+ *
+ * Allocation-free evaluation for callers that cannot let a library allocate
+ * device memory: code running while a stream is captured into a CUDA graph
+ * (cudaMalloc is illegal during capture), code that must not synchronise the
+ * device (cudaMalloc and cudaFree can), and hosts whose memory pool owns the
+ * whole GPU.  Same inputs and meaning as mtp_compute_device, outputs energy [1],
+ * forces [natoms][3] and the LAMMPS virial [6] (device pointers).  It calls no
+ * cudaMalloc, cudaFree or allocating library routine: its scratch is one
+ * fixed array of about 8.5 MB in the library's device memory, held by every
+ * GPU that loads the library until the process exits, and it uses only the
+ * contraction schedules the handle already uploaded.  Limits: at most
+ * MTP_NOALLOC_MAX_ATOMS atoms and MTP_NOALLOC_MAX_SLOTS neighbour slots
+ * (natoms * nbr_stride); larger inputs, or a basis whose value space does
+ * not fit in shared memory, return MTP_E_CAPACITY.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (several streams, several handles) race.
+ */
+#define MTP_NOALLOC_MAX_ATOMS 16384
+#define MTP_NOALLOC_MAX_SLOTS 262144
+int mtp_compute_device_noalloc(mtp_handle* h, int natoms, int nbr_stride, const int* d_itypes,
+                               const double* d_rijs, const int* d_js, const int* d_jtypes,
+                               const int* d_counts, double* d_energy, double* d_forces,
+                               double* d_virial);
+
 /* Peak FP64 / FP32 FMA throughput of device 0 measured by an FMA-chain kernel
  * (TFLOP/s, an FMA counted as 2 flops).  Used for the roofline. */
 int mtp_measure_fma_peak(double* fp64_tflops, double* fp32_tflops);

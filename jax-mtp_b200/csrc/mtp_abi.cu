@@ -14,6 +14,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -851,6 +852,163 @@ int mtp_measure_fma_peak(double* fp64, double* fp32) {
     return MTP_E_NODEVICE;
   }
   return measure_fma_peak(fp64, fp32) == cudaSuccess ? MTP_OK : MTP_E_CUDA;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Allocation-free evaluation (mtp_compute_device_noalloc)
+// ===========================================================================
+// Some callers cannot let a library call cudaMalloc: code that runs while a
+// CUDA stream is being captured into a graph (allocation is illegal there),
+// code that must not synchronise the device (cudaMalloc/cudaFree may), and
+// hosts whose memory pool owns the whole device.  This variant of
+// mtp_compute_device keeps every piece of its scratch memory in one
+// file-scope device array of fixed size instead of handle buffers, and uses
+// only the contraction schedules the handle already uploaded.
+namespace {
+
+constexpr size_t al256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+struct NoAllocLayout {
+  size_t grad, energy, wown, in_cnt, in_ptr, in_cursor, in_slot, blk, partials, tot, total;
+};
+
+constexpr NoAllocLayout noalloc_layout() {
+  NoAllocLayout L{};
+  const size_t atoms = MTP_NOALLOC_MAX_ATOMS, slots = MTP_NOALLOC_MAX_SLOTS;
+  size_t o = 0;
+  L.grad = o;      o = al256(o + slots * 3 * sizeof(double));
+  L.energy = o;    o = al256(o + atoms * sizeof(double));
+  L.wown = o;      o = al256(o + atoms * 6 * sizeof(double));
+  L.in_cnt = o;    o = al256(o + atoms * sizeof(int));
+  L.in_ptr = o;    o = al256(o + (atoms + 1) * sizeof(int));
+  L.in_cursor = o; o = al256(o + atoms * sizeof(int));
+  L.in_slot = o;   o = al256(o + slots * sizeof(int));
+  L.blk = o;       o = al256(o + (atoms / 1024 + 2) * sizeof(int));
+  L.partials = o;  o = al256(o + 7 * kReduceBlocks * sizeof(double));
+  L.tot = o;       o = al256(o + 8 * sizeof(double));
+  L.total = o;
+  return L;
+}
+
+constexpr NoAllocLayout kNoAlloc = noalloc_layout();
+
+// The scratch (about 8.5 MB).  Every GPU that loads this library holds it
+// until the process exits; all calls on a device share it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAlloc.total];
+
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the symbol is only a host-side stand-in, so the address is asked for once
+// per device (with that device current) and cached.
+int noalloc_base(mtp_handle* h, unsigned char** out) {
+  static std::mutex mu;
+  static unsigned char* base[64] = {};
+  int dev = -1;
+  MTP_CUDA(h, cudaGetDevice(&dev));
+  if (dev != h->device) return fail(h, MTP_E_INVALID, "the current CUDA device is not the handle's device");
+  if (dev < 0 || dev >= 64) return fail(h, MTP_E_INVALID, "device ordinal above 63");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!base[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return cuda_fail(h, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    base[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = base[dev];
+  return MTP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mtp_compute_device_noalloc(mtp_handle* h, int natoms, int stride, const int* d_itypes, const double* d_rijs,
+                               const int* d_js, const int* d_jtypes, const int* d_counts, double* d_energy,
+                               double* d_forces, double* d_virial) {
+  if (!h) return MTP_E_INVALID;
+  if (natoms < 0 || stride <= 0) return fail(h, MTP_E_INVALID, "natoms must be >= 0 and nbr_stride > 0");
+  if (natoms > MTP_NOALLOC_MAX_ATOMS)
+    return fail(h, MTP_E_CAPACITY, "natoms " + std::to_string(natoms) + " exceeds the allocation-free limit of " +
+                                        std::to_string(MTP_NOALLOC_MAX_ATOMS) + " atoms");
+  if (static_cast<long long>(natoms) * stride > MTP_NOALLOC_MAX_SLOTS)
+    return fail(h, MTP_E_CAPACITY, "natoms * nbr_stride exceeds the allocation-free limit of " +
+                                        std::to_string(MTP_NOALLOC_MAX_SLOTS) + " neighbour slots");
+  if (stride > h->max_nbr) return fail(h, MTP_E_CAPACITY, "nbr_stride exceeds max_nbr");
+  if (natoms > 0 && (!d_itypes || !d_rijs || !d_js || !d_jtypes || !d_forces || !d_energy || !d_virial))
+    return fail(h, MTP_E_INVALID, "null pointer");
+  unsigned char* base = nullptr;
+  int st = noalloc_base(h, &base);
+  if (st != MTP_OK) return st;
+  const bool fp64 = h->precision == MTP_PRECISION_FP64;
+
+  // launch shape from the schedules already on the device; the value space
+  // must fit in shared memory (its global-memory form would need an allocation)
+  const DeviceSchedule* ds = nullptr;
+  int lanes = 0, A = 1, bps = 0, best = -1;
+  for (const auto& kv : h->scheds) {
+    const DevModel md = make_model(h, kv.second);
+    for (int a : {4, 2, 1}) {
+      if (!eval_variant_exists(fp64, false, a)) continue;
+      const int b = eval_blocks_per_sm(md, stride, kv.first, fp64, false, a);
+      if (b <= 0) continue;
+      const int score = (a * b) * 1024 + b * kv.first / 32;
+      if (score > best) {
+        best = score;
+        ds = &kv.second;
+        lanes = kv.first;
+        A = a;
+        bps = b;
+      }
+    }
+  }
+  if (!ds)
+    return fail(h, MTP_E_CAPACITY,
+                "the value space of this basis does not fit in shared memory; the allocation-free path cannot "
+                "place it in global memory");
+
+  double* grad = reinterpret_cast<double*>(base + kNoAlloc.grad);
+  double* energy = reinterpret_cast<double*>(base + kNoAlloc.energy);
+  double* wown = reinterpret_cast<double*>(base + kNoAlloc.wown);
+  int* in_cnt = reinterpret_cast<int*>(base + kNoAlloc.in_cnt);
+  int* in_ptr = reinterpret_cast<int*>(base + kNoAlloc.in_ptr);
+  int* in_cursor = reinterpret_cast<int*>(base + kNoAlloc.in_cursor);
+  int* in_slot = reinterpret_cast<int*>(base + kNoAlloc.in_slot);
+  int* blk = reinterpret_cast<int*>(base + kNoAlloc.blk);
+  double* partials = reinterpret_cast<double*>(base + kNoAlloc.partials);
+  double* tot = reinterpret_cast<double*>(base + kNoAlloc.tot);
+
+  // The array keeps the previous call's contents.  The incoming-slot counters
+  // must start at zero (launch_incoming clears in_cnt and in_cursor first);
+  // every other piece is fully rewritten before it is read: each slot's
+  // gradient (zero for skipped slots), each site energy and per-atom virial,
+  // the scan blocks, the partials and the totals.
+  DevModel md = make_model(h, *ds);
+  DevIO io{};
+  io.natoms = natoms;
+  io.nbr_stride = stride;
+  io.n_pad = stride;
+  io.itypes = d_itypes;
+  io.rijs = d_rijs;
+  io.jtypes = d_jtypes;
+  io.counts = d_counts;
+  io.site_energy = energy;
+  io.pair_grad = grad;
+  io.err = h->d_err;
+  io.vscratch = nullptr;
+  const long long groups = (static_cast<long long>(natoms) + A - 1) / A;
+  const int blocks = static_cast<int>(std::max(1LL, std::min<long long>(static_cast<long long>(bps) * h->sm_count,
+                                                                         groups)));
+  MTP_CUDA(h, launch_incoming(natoms, stride, d_js, d_jtypes, d_counts, in_cnt, in_ptr, in_cursor, in_slot, blk,
+                              h->stream));
+  MTP_CUDA(h, launch_eval(md, io, lanes, blocks, fp64, false, A, h->stream));
+  MTP_CUDA(h, launch_force_gather(natoms, stride, d_rijs, d_counts, grad, in_ptr, in_slot, d_forces, wown, nullptr,
+                                  h->stream));
+  MTP_CUDA(h, launch_totals(natoms, energy, wown, partials, tot, h->stream));
+  MTP_CUDA(h, cudaMemcpyAsync(d_energy, tot, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  MTP_CUDA(h, cudaMemcpyAsync(d_virial, tot + 1, 6 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  h->calls++;
+  return MTP_OK;
 }
 
 }  // extern "C"

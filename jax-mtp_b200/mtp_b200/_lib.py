@@ -18,6 +18,7 @@ STATUS = {0: "MTP_OK", 1: "MTP_E_INVALID", 2: "MTP_E_FORMAT", 3: "MTP_E_CAPACITY
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 EFLAG, VFLAG, EATOM, VATOM, REUSE_NEIGHBORS = 1, 2, 4, 8, 16
+NOALLOC_MAX_ATOMS, NOALLOC_MAX_SLOTS = 16384, 262144
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -49,6 +50,7 @@ SIGNATURES = {
     "mtp_verlet_device": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _D, _I]),
     "mtp_profile": (_I, [_P, _I]),
     "mtp_profile_read": (_I, [_P, ctypes.POINTER(_D), ctypes.POINTER(_I)]),
+    "mtp_compute_device_noalloc": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
 }
 
 _lib = None

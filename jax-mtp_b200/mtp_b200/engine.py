@@ -314,3 +314,24 @@ MTPEngine.pack_rij_device = _pack_rij_device
 MTPEngine.verlet_device = _verlet_device
 MTPEngine.profile = _profile
 MTPEngine.profile_read = _profile_read
+
+
+def _compute_device_noalloc(self, itypes, rijs, js, jtypes, counts, energy, forces, virial, stream=None):
+    """mtp_compute_device_noalloc: the evaluation with no device allocation at all.
+
+    For callers that cannot allocate device memory (inside CUDA-graph capture,
+    under an external memory pool, or where an allocation's implicit device
+    synchronisation is not allowed).  Outputs must be preallocated device
+    tensors: energy [1], forces [N, 3], virial [6] (float64).  Calls that
+    overlap on the GPU share one scratch array and race.
+    """
+    import torch
+    st = torch.cuda.current_stream(rijs.device) if stream is None else stream
+    self.set_stream(st.cuda_stream)
+    code = lib().mtp_compute_device_noalloc(self._h, int(itypes.shape[0]), int(rijs.shape[1]), _tp(itypes),
+                                             _tp(rijs), _tp(js), _tp(jtypes), _tp(counts), _tp(energy), _tp(forces),
+                                             _tp(virial))
+    check(code, self._h)
+
+
+MTPEngine.compute_device_noalloc = _compute_device_noalloc

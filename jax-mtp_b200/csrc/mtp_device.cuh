@@ -83,7 +83,7 @@ constexpr int kPrefetch = 8;
 // atoms; neighbour staging is kept per atom.
 struct SmemLayout {
   int pws;        // stride of a power row (3 (D+1), rounded up to odd)
-  size_t v, rad, u, f, fp, pw, slot, abc, mk, red, cnt, total;
+  size_t v, rad, u, f, fp, pw, slot, abc, mk, dmt, red, cnt, total;
 };
 
 template <typename T>
@@ -107,6 +107,7 @@ __host__ __device__ inline SmemLayout smem_layout(int v_size, int S, int R, int 
   L.slot = take(sizeof(int) * n_pad * A);
   L.abc = take(sizeof(int) * 4 * P);
   L.mk = take(sizeof(int) * kMaxR * P);
+  L.dmt = take(sizeof(T) * R * P * A);
   L.red = take(sizeof(double) * (threads / 32) * A);
   L.cnt = take(sizeof(int) * (threads / 32 + 1));
   L.total = (o + 31) & ~size_t(31);
@@ -387,6 +388,7 @@ __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
         T acc[kMaxR];
 #pragma unroll
         for (int mu = 0; mu < kMaxR; ++mu) acc[mu] = T(0);
+#pragma unroll 4
         for (int q = 0; q < nv; ++q) {
           const T* pw = sPw + q * pws;
           const T mono = pw[ea] * pw[D1 + eb] * pw[2 * D1 + ec];
@@ -446,6 +448,14 @@ __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
     }
 
     // ---- N3: dE_i/dr_ij per kept neighbour -------------------------------
+    // dense table D[a][p][mu] = dE/dm of basic moment (mu, p) (0 if absent)
+    T* sDm = reinterpret_cast<T*>(smem + L.dmt);
+    for (int x = tid; x < P * R * A; x += NT) {
+      const int a = x / (P * R), pm = x % (P * R);
+      const int k = sMk[kMaxR * (pm / R) + pm % R];
+      sDm[x] = k >= 0 ? V[(md.v_dm + k) * A + a] : T(0);
+    }
+    __syncthreads();
 #pragma unroll
     for (int a = 0; a < A; ++a) {
       const int atom = base + a;
@@ -473,18 +483,19 @@ __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
             fp[mu] = mu < R ? sFp[q * R + mu] : T(0);
           }
           const T* pw = sPw + q * pws;
+          const T* dmt = sDm + static_cast<size_t>(a) * P * R;
+#pragma unroll 2
           for (int p = sl; p < P; p += tpn) {
-            const int ea = sAbc[4 * p], eb = sAbc[4 * p + 1], ec = sAbc[4 * p + 2];
+            const int4 abc = *reinterpret_cast<const int4*>(sAbc + 4 * p);
+            const int ea = abc.x, eb = abc.y, ec = abc.z;
+            const T* drow = dmt + p * R;
             T W = T(0), Wp = T(0);
 #pragma unroll
             for (int mu = 0; mu < kMaxR; ++mu) {
               if (mu < R) {
-                const int k = sMk[kMaxR * p + mu];
-                if (k >= 0) {
-                  const T g = V[(md.v_dm + k) * A + a];
-                  W = dev_fma(g, f[mu], W);
-                  Wp = dev_fma(g, fp[mu], Wp);
-                }
+                const T g = drow[mu];
+                W = dev_fma(g, f[mu], W);
+                Wp = dev_fma(g, fp[mu], Wp);
               }
             }
             const T px = pw[ea], py = pw[D1 + eb], pz = pw[2 * D1 + ec];

@@ -304,6 +304,17 @@ def run_ours(args):
     counts_real = valid.sum(1).cpu().numpy()
     flops = algorithmic_flops(pot, counts_real)
 
+    # launch shapes by the autotuner (timed on these rows)
+    from mtp_b200.autotune import tune
+    tuning = {}
+    for p in ("mixed", "fp64"):
+        md = mds[p]
+        r = tune(eng[p], md.types, md.rijs, md.js, md.jtypes, md.counts, use_cache=False)
+        tuning[p] = {"threads": r["threads"], "atoms_per_block": r["atoms_per_block"],
+                     "eval_ms": r["ms"], "ran": r["ran"]}
+        md._forces(reuse=False)       # rebuild the incoming lists after tuning
+    torch.cuda.synchronize(device)
+    e_start = {p: mds[p].total_energy() for p in ("mixed", "fp64")}
     for p in ("mixed", "fp64"):
         mds[p].capture()
     # timed regions
@@ -324,6 +335,12 @@ def run_ours(args):
         results[p]["eval_ms_per_launch"] = kms / max(1, kn)
         results[p]["eval_launches"] = kn
     clocks = sampler.summary()
+    # NVE drift over warm-up + timed steps (graph replays), per precision
+    drift = {}
+    for p in ("mixed", "fp64"):
+        nsteps = mds[p].step_count
+        e_end = mds[p].total_energy()
+        drift[p] = {"steps": nsteps, "meV_per_atom_per_ps": (e_end - e_start[p]) / N * 1e3 / (nsteps * DT)}
     for p in ("mixed", "fp64"):
         mds[p].release()
     # drift over the timed run (energy per atom)
@@ -350,6 +367,11 @@ def run_ours(args):
 
     for p in ("mixed", "fp64"):
         eng[p].close()
+    del mds
+    torch.cuda.empty_cache()
+    train = None
+    if not args.skip_train:
+        train = run_train(args, device, dist)
 
     if rank == 0:
         line = {
@@ -360,6 +382,9 @@ def run_ours(args):
             "fp64": {"value": value64, "unit": "atom-steps/s", "ms_per_step": results["fp64"]["ms"] / args.steps},
             "mixed_over_fp64": value / value64,
             "force_error_mixed_vs_fp64": force_err,
+            "nve_drift": drift,
+            "autotuned_launch": tuning,
+            "train": train,
             "roofline": {"bound": "fp32-fma", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
                          "kernel": "k_mtp_eval<float> (mixed)", "flops_per_launch": flops,
@@ -378,6 +403,99 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def run_train(args, device, dist):
+    """Training throughput: configuration 3 (level 20, 2 species, 512 periodic
+    configurations, N in [16, 256], batched forward in mixed precision) and
+    configuration 4 (level 28, 4 species, 256 configurations, N in [32, 512],
+    FP64 forward + hand-written adjoint of the E/F/stress loss)."""
+    import torch
+    from mtp_b200 import synth
+    from mtp_b200.engine import MTPEngine
+    from mtp_b200.mtp_file import read_mtp
+    from mtp_b200.train import DeviceBatch, predict, weighted_loss
+    potdir = os.path.join(ROOT, "tests", "golden", "potentials")
+    out = {}
+
+    def timed(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize(device)
+        if dist is not None:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(device)
+        return max_over_ranks(e0.elapsed_time(e1), dist, device)
+
+    world = 1 if dist is None else dist.get_world_size()
+    # ---- configuration 3: batched forward, mixed precision
+    pot3 = read_mtp(os.path.join(potdir, "cfg3_L20_S2.mtp"))
+    structs = synth.training_batch(512, 16, 256, 2, seed=6)
+    nds = [synth.build_neighbors(st, pot3.max_dist) for st in structs]
+    nd, cfg, offs, vols = synth.pack_batch(nds)
+    batch = DeviceBatch.from_numpy(nd, cfg, vols, device=device)
+    with MTPEngine(os.path.join(potdir, "cfg3label_L20_S2.mtp"), nd.natoms, nd.n_pad) as lab:
+        E_l, F_l, S_l = lab.batch_device(batch.itypes, batch.rijs, batch.js, batch.jtypes, batch.counts, batch.cfg,
+                                         batch.volumes, batch.nconfig)
+    g = torch.Generator(device="cpu").manual_seed(7)
+    natom_c = torch.as_tensor(np.diff(offs), dtype=torch.float64, device=device)
+    E_t = E_l + 1e-3 * natom_c * torch.randn(batch.nconfig, generator=g, dtype=torch.float64).to(device)
+    F_t = F_l + 1e-2 * torch.randn(F_l.shape, generator=g, dtype=torch.float64).to(device)
+    S_t = S_l + 6.2415e-4 * torch.randn(S_l.shape, generator=g, dtype=torch.float64).to(device)
+    with MTPEngine(os.path.join(potdir, "cfg3_L20_S2.mtp"), nd.natoms, nd.n_pad, precision="mixed") as eng3:
+        def fwd3():
+            eng3.batch_device(batch.itypes, batch.rijs, batch.js, batch.jtypes, batch.counts, batch.cfg,
+                              batch.volumes, batch.nconfig)
+        steps = max(3, min(args.steps, 10))
+        ms = timed(fwd3, steps, 3)
+        E_p, F_p, S_p = eng3.batch_device(batch.itypes, batch.rijs, batch.js, batch.jtypes, batch.counts, batch.cfg,
+                                          batch.volumes, batch.nconfig)
+        loss = float(weighted_loss(E_p, F_p, S_p, (E_t, F_t, S_t)))
+        eng3.sync_status()
+    out["cfg3_batched_forward"] = {"value": world * batch.nconfig * steps / (ms * 1e-3), "unit": "cfg/s",
+                                   "configs": batch.nconfig, "atoms": batch.natoms, "nbr_stride": nd.n_pad,
+                                   "ms_per_batch": ms / steps, "precision": "mixed", "loss_vs_labels": loss,
+                                   "labels": "second random level-20 MTP (seed 7) + noise 1 meV/atom, "
+                                             "10 meV/A, 0.1 GPa"}
+    del batch
+    # ---- configuration 4: forward + adjoint training step, FP64
+    pot4 = read_mtp(os.path.join(potdir, "cfg4_L28_S4.mtp"))
+    structs = synth.training_batch(256, 32, 512, 4, seed=8)
+    nds = [synth.build_neighbors(st, pot4.max_dist) for st in structs]
+    nd, cfg, offs, vols = synth.pack_batch(nds)
+    batch = DeviceBatch.from_numpy(nd, cfg, vols, device=device)
+    with MTPEngine(os.path.join(potdir, "cfg4_L28_S4.mtp"), nd.natoms, nd.n_pad, precision="fp64") as eng4:
+        params = {k: torch.tensor(v, dtype=torch.float64, device=device, requires_grad=True)
+                  for k, v in (("species", pot4.species_coeffs), ("basis", pot4.moment_coeffs),
+                               ("radial", pot4.radial_coeffs))}
+        with torch.no_grad():
+            E0, F0, S0 = predict(params, eng4, batch)
+        g = torch.Generator(device="cpu").manual_seed(9)
+        tgt = (E0 + 1e-3 * torch.randn(E0.shape, generator=g, dtype=torch.float64).to(device),
+               F0 + 1e-2 * torch.randn(F0.shape, generator=g, dtype=torch.float64).to(device),
+               S0 + 6.2415e-4 * torch.randn(S0.shape, generator=g, dtype=torch.float64).to(device))
+
+        def step4():
+            for v in params.values():
+                v.grad = None
+            L = weighted_loss(*predict(params, eng4, batch), tgt)
+            L.backward()
+
+        steps = max(2, min(args.steps, 4))
+        ms = timed(step4, steps, 1)
+        eng4.sync_status()
+    out["cfg4_train_step"] = {"value": world * batch.nconfig * steps / (ms * 1e-3), "unit": "cfg/s",
+                              "configs": batch.nconfig, "atoms": batch.natoms, "nbr_stride": nd.n_pad,
+                              "ms_per_step": ms / steps, "precision": "fp64",
+                              "step": "batched forward (E, F, stress) + loss + hand-written adjoint w.r.t. all "
+                                      "coefficients", "jax_grad_baseline": "unavailable on this box (no JAX)"}
+    return out
 
 
 def run_e2e(eng, md, N, args):
@@ -434,6 +552,7 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--skip-train", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

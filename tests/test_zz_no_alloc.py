@@ -20,7 +20,10 @@ from mtp_b200 import _lib
 from mtp_b200.engine import MTPEngine
 
 pytestmark = pytest.mark.gpu
-REL = 1e-10
+# FP64: the bar of every FP64 parity test.  Mixed: both entry points may pick
+# different launch shapes (summation orders) in FP32, so the bar is the FP32
+# rounding level, far inside the mixed error budget (0.1 meV/atom, 1 meV/A).
+REL = {"fp64": 1e-10, "mixed": 1e-5}
 
 
 def _rel(a, b):
@@ -51,9 +54,10 @@ def test_noalloc_matches_regular_entry_point_twice(tag, precision):
             eng.compute_device_noalloc(it, rij, js, jt, cnt, E, F, W)
             torch.cuda.synchronize()
             eng.sync_status()
-            assert abs(float(E.cpu()[0]) - ref[0]) <= REL * abs(ref[0])
-            assert _rel(F.cpu().numpy(), ref[1]) <= REL
-            assert _rel(W.cpu().numpy(), ref[2]) <= REL
+            tol = REL[precision]
+            assert abs(float(E.cpu()[0]) - ref[0]) <= tol * abs(ref[0])
+            assert _rel(F.cpu().numpy(), ref[1]) <= tol
+            assert _rel(W.cpu().numpy(), ref[2]) <= tol
 
 
 def test_noalloc_rejects_inputs_above_its_limits():

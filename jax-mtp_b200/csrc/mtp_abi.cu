@@ -146,13 +146,19 @@ DevModel make_model(mtp_handle* h, const DeviceSchedule& ds) {
   return md;
 }
 
-// Schedule for `lanes`, built and uploaded on first use.
-int get_schedule(mtp_handle* h, int lanes, DeviceSchedule** out) {
-  auto it = h->scheds.find(lanes);
+// Bytes of one operand access of the evaluation kernel (sets the bank model
+// the schedule's entry order is tuned for).
+inline int access_width(bool fp64, int atoms_per_block) { return (fp64 ? 8 : 4) * atoms_per_block; }
+
+// Schedule for `lanes` threads and `width`-byte operand accesses, built and
+// uploaded on first use.
+int get_schedule(mtp_handle* h, int lanes, int width, DeviceSchedule** out) {
+  const int key = lanes * 64 + width;
+  auto it = h->scheds.find(key);
   if (it == h->scheds.end()) {
     DeviceSchedule ds;
     std::string err;
-    if (!build_schedule(h->pot, lanes, ds.sched, err)) return fail(h, MTP_E_FORMAT, err);
+    if (!build_schedule(h->pot, lanes, ds.sched, err, width)) return fail(h, MTP_E_FORMAT, err);
     const auto& ent = ds.sched.entries;
     MTP_CUDA(h, dalloc(&ds.d_entries, ent.size() / 2));
     MTP_CUDA(h, cudaMemcpy(ds.d_entries, ent.data(), ent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
@@ -168,7 +174,7 @@ int get_schedule(mtp_handle* h, int lanes, DeviceSchedule** out) {
         MTP_CUDA(h, cudaMemcpy(h->d_zero, ds.sched.zero_list.data(), ds.sched.zero_list.size() * sizeof(int),
                                cudaMemcpyHostToDevice));
     }
-    it = h->scheds.emplace(lanes, ds).first;
+    it = h->scheds.emplace(key, ds).first;
   }
   *out = &it->second;
   return MTP_OK;
@@ -235,12 +241,12 @@ int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, 
     else a_c = {4, 2, 1};
     int best = -1;
     for (int lanes : lanes_c) {
-      DeviceSchedule* ds = nullptr;
-      int st = get_schedule(h, lanes, &ds);
-      if (st != MTP_OK) return st;
-      const DevModel md = make_model(h, *ds);
       for (int A : a_c) {
         if (!eval_variant_exists(fp64, false, A)) continue;
+        DeviceSchedule* ds = nullptr;
+        int st = get_schedule(h, lanes, access_width(fp64, A), &ds);
+        if (st != MTP_OK) return st;
+        const DevModel md = make_model(h, *ds);
         int bps = eval_blocks_per_sm(md, stride, lanes, fp64, false, A);
         if (h->blocks_per_sm > 0) bps = std::min(bps, h->blocks_per_sm);
         if (bps <= 0) continue;
@@ -253,7 +259,7 @@ int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, 
     }
     if (best < 0) {
       DeviceSchedule* ds = nullptr;
-      int st = get_schedule(h, h->threads, &ds);
+      int st = get_schedule(h, h->threads, access_width(fp64, 1), &ds);
       if (st != MTP_OK) return st;
       int bps = eval_blocks_per_sm(make_model(h, *ds), stride, h->threads, fp64, true, 1);
       if (h->blocks_per_sm > 0) bps = std::min(bps, h->blocks_per_sm);
@@ -262,13 +268,13 @@ int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, 
       c = mtp_handle::LaunchChoice{h->threads, bps, true, 0, 1};
     }
     DeviceSchedule* ds = nullptr;
-    int st = get_schedule(h, c.lanes, &ds);
+    int st = get_schedule(h, c.lanes, access_width(fp64, c.A), &ds);
     if (st != MTP_OK) return st;
     c.smem = eval_smem_bytes(make_model(h, *ds), stride, c.lanes, fp64, c.vglobal, c.A);
     h->launch_cache[key] = c;
   }
   DeviceSchedule* ds = nullptr;
-  int st = get_schedule(h, c.lanes, &ds);
+  int st = get_schedule(h, c.lanes, access_width(fp64, c.A), &ds);
   if (st != MTP_OK) return st;
   const long long groups = (static_cast<long long>(natoms) + c.A - 1) / c.A;
   const long long blocks = std::max(1LL, std::min<long long>(static_cast<long long>(c.bps) * h->sm_count, groups));
@@ -472,7 +478,7 @@ int mtp_create(const char* mtp_path, int max_atoms, int max_nbr, double cutoff, 
   int st = upload_coeffs(h);
   if (st != MTP_OK) return bail(st);
   DeviceSchedule* ds = nullptr;
-  st = get_schedule(h, h->threads, &ds);
+  st = get_schedule(h, h->threads, access_width(precision == MTP_PRECISION_FP64, 1), &ds);
   if (st != MTP_OK) return bail(st);
   if (h->debug >= 1) {
     std::fprintf(stderr, "[mtp_b200] %s: S=%d R=%d K=%d M=%d B=%d T=%d Sa=%d; %d fwd + %d rev passes, %d value slots\n",
@@ -722,7 +728,7 @@ int mtp_adjoint_batch_device(mtp_handle* h, int natoms, int stride, int nconfig,
   if (natoms > 0 && (!d_itypes || !d_rijs || !d_js || !d_jtypes || !d_cfg || !d_volumes || !d_gE || !d_gF || !d_gS))
     return fail(h, MTP_E_INVALID, "null pointer");
   DeviceSchedule* ds = nullptr;
-  int st = get_schedule(h, h->threads, &ds);
+  int st = get_schedule(h, h->threads, access_width(true, 1), &ds);
   if (st != MTP_OK) return st;
   DevModel md = make_model(h, *ds);
   TrainIO tio{};
@@ -948,15 +954,16 @@ int mtp_compute_device_noalloc(mtp_handle* h, int natoms, int stride, const int*
   int lanes = 0, A = 1, bps = 0, best = -1;
   for (const auto& kv : h->scheds) {
     const DevModel md = make_model(h, kv.second);
+    const int sl = kv.second.sched.lanes;
     for (int a : {4, 2, 1}) {
       if (!eval_variant_exists(fp64, false, a)) continue;
-      const int b = eval_blocks_per_sm(md, stride, kv.first, fp64, false, a);
+      const int b = eval_blocks_per_sm(md, stride, sl, fp64, false, a);
       if (b <= 0) continue;
-      const int score = (a * b) * 1024 + b * kv.first / 32;
+      const int score = (a * b) * 1024 + b * sl / 32;
       if (score > best) {
         best = score;
         ds = &kv.second;
-        lanes = kv.first;
+        lanes = sl;
         A = a;
         bps = b;
       }

@@ -129,14 +129,9 @@ struct __align__(sizeof(T) * A) Pack {
 // [steps][lanes] entry array with kPrefetch entries in flight (registers), so
 // the L2 latency of the program overlaps the arithmetic.  Each entry feeds A
 // atoms: acc[a] += c * V[x][a] * V[y][a]; STORE/ADD flush into V[d][a].
-// The operands of step s+1 are loaded before step s flushes: no lane of a pass
-// reads a slot that any lane writes in the same pass (a property of the
-// schedule), so the next loads never depend on the store, and their shared-
-// memory latency leaves the per-step critical path.
 template <typename T, int A>
 __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int steps, int lanes, int tid,
                                          T* __restrict__ V) {
-  if (steps <= 0) return;
   const uint2* p = ent + tid;
   uint2 buf[kPrefetch];
 #pragma unroll
@@ -144,30 +139,21 @@ __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int step
   T acc[A];
 #pragma unroll
   for (int a = 0; a < A; ++a) acc[a] = T(0);
-  uint2 e_cur = buf[0];
-  if (kPrefetch < steps) buf[0] = __ldg(p + static_cast<size_t>(kPrefetch) * lanes);
-  Pack<T, A> va_cur = *reinterpret_cast<const Pack<T, A>*>(V + (e_cur.x & 0xFFFFu) * A);
-  Pack<T, A> vb_cur = *reinterpret_cast<const Pack<T, A>*>(V + (e_cur.x >> 16) * A);
   for (int s0 = 0; s0 < steps; s0 += kPrefetch) {
 #pragma unroll
     for (int k = 0; k < kPrefetch; ++k) {
-      const int s = s0 + k;
-      if (s < steps) {
-        const int kn = (k + 1) % kPrefetch;
-        uint2 e_nxt = buf[kn];
-        Pack<T, A> va_nxt, vb_nxt;
-        if (s + 1 < steps) {
-          const int nx = s + 1 + kPrefetch;
-          if (nx < steps) buf[kn] = __ldg(p + static_cast<size_t>(nx) * lanes);
-          va_nxt = *reinterpret_cast<const Pack<T, A>*>(V + (e_nxt.x & 0xFFFFu) * A);
-          vb_nxt = *reinterpret_cast<const Pack<T, A>*>(V + (e_nxt.x >> 16) * A);
-        }
-        const T c = static_cast<T>(e_cur.y >> 18);
+      if (s0 + k < steps) {
+        const uint2 e = buf[k];
+        const int nx = s0 + k + kPrefetch;
+        if (nx < steps) buf[k] = __ldg(p + static_cast<size_t>(nx) * lanes);
+        const T c = static_cast<T>(e.y >> 18);
+        const Pack<T, A> va = *reinterpret_cast<const Pack<T, A>*>(V + (e.x & 0xFFFFu) * A);
+        const Pack<T, A> vb = *reinterpret_cast<const Pack<T, A>*>(V + (e.x >> 16) * A);
 #pragma unroll
-        for (int a = 0; a < A; ++a) acc[a] = dev_fma(c * va_cur.v[a], vb_cur.v[a], acc[a]);
-        const uint32_t op = (e_cur.y >> 16) & 3u;
+        for (int a = 0; a < A; ++a) acc[a] = dev_fma(c * va.v[a], vb.v[a], acc[a]);
+        const uint32_t op = (e.y >> 16) & 3u;
         if (op) {
-          Pack<T, A>* dst = reinterpret_cast<Pack<T, A>*>(V + (e_cur.y & 0xFFFFu) * A);
+          Pack<T, A>* dst = reinterpret_cast<Pack<T, A>*>(V + (e.y & 0xFFFFu) * A);
           Pack<T, A> out;
           if (op == kOpStore) {
 #pragma unroll
@@ -181,9 +167,6 @@ __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int step
 #pragma unroll
           for (int a = 0; a < A; ++a) acc[a] = T(0);
         }
-        e_cur = e_nxt;
-        va_cur = va_nxt;
-        vb_cur = vb_nxt;
       }
     }
   }

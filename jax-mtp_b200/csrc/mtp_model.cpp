@@ -253,8 +253,20 @@ struct RawPass {
   std::vector<RawEntry> e;  // [steps][lanes]
 };
 
-// Lay jobs onto lanes (longest first onto the least loaded lane).
-RawPass lay_out(const std::vector<Job>& jobs, int lanes) {
+// Lay jobs onto lanes (longest first onto the least loaded lane), then order
+// the entries step by step so that the lanes sharing a shared-memory
+// wavefront read operands in different banks.  A warp's two operand gathers
+// of a step are two shared-memory instructions; each costs as many wavefronts
+// as the most distinct addresses any bank receives.  With `width`-byte
+// accesses, 128 / width consecutive lanes share a wavefront and the bank key
+// of value slot x is x mod (128 / width).  Within a job the entries may come
+// in any order (the sum is fixed by the schedule, so still deterministic), and
+// with `allow_swap` the two operands of a product may trade places; the
+// greedy picks, lane by lane, the entry (among the first kWindow remaining)
+// that adds the fewest conflicts, and the last entry of a job carries its
+// flush.
+RawPass lay_out(const std::vector<Job>& jobs, int lanes, int width, bool allow_swap) {
+  constexpr size_t kWindow = 32;
   std::vector<int> order(jobs.size());
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(),
@@ -278,20 +290,81 @@ RawPass lay_out(const std::vector<Job>& jobs, int lanes) {
   }
   p.steps = static_cast<int>(steps);
   p.e.assign(steps * lanes, RawEntry{kSymZero, kSymZero, kSymZero, kOpNone, 0});
-  for (int l = 0; l < lanes; ++l) {
-    size_t s = 0;
-    for (int j : lane_jobs[l]) {
-      const Job& jb = jobs[j];
-      for (size_t k = 0; k < jb.sides.size(); ++k, ++s) {
+
+  struct LaneState {
+    size_t next_job = 0;
+    int job = -1;
+    std::vector<Side> rem;
+  };
+  std::vector<LaneState> st(lanes);
+  auto advance = [&](int l) {
+    LaneState& L = st[l];
+    while (L.rem.empty() && L.next_job < lane_jobs[l].size()) {
+      L.job = lane_jobs[l][L.next_job++];
+      L.rem = jobs[L.job].sides;
+    }
+    return !L.rem.empty();
+  };
+  const int group = std::max(1, std::min(32, 128 / std::max(4, width)));
+  const uint32_t nkey = static_cast<uint32_t>(group);
+  std::vector<std::vector<uint32_t>> usedA(nkey), usedB(nkey);
+  auto symbolic = [](uint32_t x) { return x == kSymZero || x == kSymOne; };
+  auto load = [&](const std::vector<std::vector<uint32_t>>& used, uint32_t x) -> size_t {
+    if (symbolic(x)) return 0;   // one shared constant slot: every lane reads the same address
+    const auto& v = used[x % nkey];
+    for (uint32_t y : v)
+      if (y == x) return 0;
+    return v.size();
+  };
+  auto mark = [&](std::vector<std::vector<uint32_t>>& used, uint32_t x) {
+    if (symbolic(x)) return;
+    auto& v = used[x % nkey];
+    for (uint32_t y : v)
+      if (y == x) return;
+    v.push_back(x);
+  };
+  for (size_t s = 0; s < steps; ++s) {
+    for (int g0 = 0; g0 < lanes; g0 += group) {
+      for (auto& v : usedA) v.clear();
+      for (auto& v : usedB) v.clear();
+      for (int l = g0; l < std::min(lanes, g0 + group); ++l) {
+        if (!advance(l)) continue;   // padding entry (constant-zero slot)
+        LaneState& L = st[l];
+        size_t best = 0, best_cost = SIZE_MAX;
+        bool best_swap = false;
+        const size_t ncand = std::min(kWindow, L.rem.size());
+        for (size_t i = 0; i < ncand && best_cost > 0; ++i) {
+          const Side& c = L.rem[i];
+          size_t cost = load(usedA, c.a) + load(usedB, c.b);
+          bool sw = false;
+          if (allow_swap) {
+            const size_t c2 = load(usedA, c.b) + load(usedB, c.a);
+            if (c2 < cost) {
+              cost = c2;
+              sw = true;
+            }
+          }
+          if (cost < best_cost) {
+            best_cost = cost;
+            best = i;
+            best_swap = sw;
+          }
+        }
+        Side c = L.rem[best];
+        if (best_swap) std::swap(c.a, c.b);
+        L.rem[best] = L.rem.back();
+        L.rem.pop_back();
+        mark(usedA, c.a);
+        mark(usedB, c.b);
         RawEntry& r = p.e[s * lanes + l];
-        r.a = jb.sides[k].a;
-        r.b = jb.sides[k].b;
-        r.c = jb.sides[k].c;
+        r.a = c.a;
+        r.b = c.b;
+        r.c = c.c;
         r.dst = kSymZero;
         r.op = kOpNone;
-        if (k + 1 == jb.sides.size()) {
-          r.dst = jb.dst;
-          r.op = jb.op;
+        if (L.rem.empty()) {
+          r.dst = jobs[L.job].dst;
+          r.op = jobs[L.job].op;
         }
       }
     }
@@ -302,7 +375,8 @@ RawPass lay_out(const std::vector<Job>& jobs, int lanes) {
 // Split long jobs into chunks writing partial slots; returns the main pass and,
 // when anything was split, the combine pass.  `parts_used` gets the number of
 // partial slots the pass pair needs.
-void emit_jobs(const std::vector<Job>& jobs, int lanes, std::vector<RawPass>& out, int& parts_used) {
+void emit_jobs(const std::vector<Job>& jobs, int lanes, int width, bool allow_swap, std::vector<RawPass>& out,
+               int& parts_used) {
   size_t total = 0;
   for (const Job& j : jobs) total += j.sides.size();
   if (total == 0) return;
@@ -327,8 +401,8 @@ void emit_jobs(const std::vector<Job>& jobs, int lanes, std::vector<RawPass>& ou
     }
     comb_jobs.push_back(std::move(comb));
   }
-  out.push_back(lay_out(main_jobs, lanes));
-  if (!comb_jobs.empty()) out.push_back(lay_out(comb_jobs, lanes));
+  out.push_back(lay_out(main_jobs, lanes, width, allow_swap));
+  if (!comb_jobs.empty()) out.push_back(lay_out(comb_jobs, lanes, width, false));
   parts_used = std::max(parts_used, parts);
 }
 
@@ -345,9 +419,10 @@ void seed_list(const Potential& pot, std::vector<int>& idx, std::vector<double>&
   }
 }
 
-bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& err) {
+bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& err, int width) {
   s = Schedule();
   s.lanes = lanes;
+  s.width = width;
   const int M = pot.M, B = pot.B, T = pot.T;
   if (lanes <= 0 || lanes % 32 != 0) { err = "lanes must be a positive multiple of 32"; return false; }
 
@@ -431,7 +506,7 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
       jobs[it->second].sides.push_back(
           Side{static_cast<uint32_t>(s.v_m + r[0]), static_cast<uint32_t>(s.v_m + r[1]), static_cast<uint32_t>(r[2])});
     }
-    emit_jobs(jobs, lanes, fwd, parts);
+    emit_jobs(jobs, lanes, width, true, fwd, parts);
   }
   // reverse: passes for target depth maxd..1 gather sides whose source has
   // depth >= 1; every side into a depth-0 source waits for one final pass.
@@ -454,7 +529,7 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
       if (depth[r[0]] >= 1) add_side(jobs, job_of, r[0], r[3], r[1], r[2]);
       if (depth[r[1]] >= 1) add_side(jobs, job_of, r[1], r[3], r[0], r[2]);
     }
-    emit_jobs(jobs, lanes, rev, parts);
+    emit_jobs(jobs, lanes, width, false, rev, parts);
   }
   {
     std::vector<Job> jobs;
@@ -467,7 +542,7 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
         if (depth[r[1]] == 0) add_side(jobs, job_of, r[1], r[3], r[0], r[2]);
       }
     }
-    emit_jobs(jobs, lanes, rev, parts);
+    emit_jobs(jobs, lanes, width, false, rev, parts);
   }
   s.n_part = parts;
   s.v_zero = s.v_part + parts;

@@ -53,6 +53,7 @@ struct Pass {
 
 struct Schedule {
   int lanes = 0;          // threads per block the programs were built for
+  int width = 4;          // bytes per operand access the entry order was tuned for
   // Value-space layout (indices into the per-atom value array V):
   int v_m = 0;            // moments m[0..M)
   int v_dm = 0;           // adjoints dE/dm[0..M)
@@ -72,9 +73,11 @@ struct Schedule {
   int max_depth = 0;
 };
 
-// Build the schedule for `lanes` threads per block.  Fails (false, err) if the
-// table does not have a write-before-read order, or exceeds index limits.
-bool build_schedule(const Potential& pot, int lanes, Schedule& out, std::string& err);
+// Build the schedule for `lanes` threads per block whose operand accesses are
+// `width` bytes (sizeof(real) x atoms per block; it sets the bank model the
+// entry order is tuned for).  Fails (false, err) if the table does not have a
+// write-before-read order, or exceeds index limits.
+bool build_schedule(const Potential& pot, int lanes, Schedule& out, std::string& err, int width = 4);
 
 // Execute the schedule for one atom on the host (bit-for-bit the device
 // arithmetic order, in double): V must have v_size entries with basic moments

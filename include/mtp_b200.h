@@ -203,9 +203,10 @@ int mtp_parse_info(const char* mtp_path, int* out8, char* err, int err_len);
  * a test hook for the table preprocessing).  basic [alpha_index_basic_count]
  * moments in, moments [alpha_moments_count] and dE/dmoment [alpha_moments_count]
  * out, using the handle-free preprocessing of the file and the schedule for
- * threads_per_block lanes.
+ * threads_per_block lanes whose entry order is tuned for access_width-byte
+ * operand loads (4, 8 or 16).
  */
-int mtp_schedule_emulate(const char* mtp_path, int threads_per_block, const double* basic,
+int mtp_schedule_emulate(const char* mtp_path, int threads_per_block, int access_width, const double* basic,
                          double* moments, double* dmoments, double* energy_part);
 
 /*

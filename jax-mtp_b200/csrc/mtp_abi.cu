@@ -385,14 +385,15 @@ int mtp_parse_info(const char* path, int* out8, char* errbuf, int err_len) {
   return MTP_OK;
 }
 
-int mtp_schedule_emulate(const char* path, int lanes, const double* basic, double* moments, double* dmoments,
-                         double* energy_part) {
+int mtp_schedule_emulate(const char* path, int lanes, int width, const double* basic, double* moments,
+                         double* dmoments, double* energy_part) {
   if (!path || !basic || !moments || !dmoments) return MTP_E_INVALID;
+  if (width != 4 && width != 8 && width != 16) return MTP_E_INVALID;
   Potential pot;
   std::string err;
   if (!parse_mtp_file(path, pot, err)) return MTP_E_FORMAT;
   Schedule s;
-  if (!build_schedule(pot, lanes, s, err)) return MTP_E_FORMAT;
+  if (!build_schedule(pot, lanes, s, err, width)) return MTP_E_FORMAT;
   std::vector<double> V(s.v_size, 0.0);
   for (int k = 0; k < pot.B; ++k) V[s.v_m + k] = basic[k];
   double e = emulate_schedule(pot, s, V);

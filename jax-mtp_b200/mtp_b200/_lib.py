@@ -43,7 +43,7 @@ SIGNATURES = {
     "mtp_set_launch": (_I, [_P, _I, _I, _I]),
     "mtp_get_launch": (_I, [_P, _P]),
     "mtp_parse_info": (_I, [ctypes.c_char_p, _P, ctypes.c_char_p, _I]),
-    "mtp_schedule_emulate": (_I, [ctypes.c_char_p, _I, _P, _P, _P, _P]),
+    "mtp_schedule_emulate": (_I, [ctypes.c_char_p, _I, _I, _P, _P, _P, _P]),
     "mtp_measure_fma_peak": (_I, [ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "mtp_neighbors_device": (_I, [_P, _I, _P, _P, _P, _D, _I, _P, _P, _P, _P]),
     "mtp_pack_rij_device": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _P]),

@@ -240,14 +240,15 @@ def parse_info(path: str) -> Dict[str, int]:
     return dict(zip(keys, (int(x) for x in out)))
 
 
-def schedule_emulate(path: str, lanes: int, basic: np.ndarray):
+def schedule_emulate(path: str, lanes: int, basic: np.ndarray, width: int = 4):
     """Run the contraction schedule on the host (test hook)."""
     info = parse_info(path)
     b = _c(basic, np.float64)
     m = np.zeros(info["alpha_moments_count"])
     dm = np.zeros(info["alpha_moments_count"])
     e = np.zeros(1)
-    code = lib().mtp_schedule_emulate(str(path).encode(), int(lanes), _ptr(b), _ptr(m), _ptr(dm), _ptr(e))
+    code = lib().mtp_schedule_emulate(str(path).encode(), int(lanes), int(width), _ptr(b), _ptr(m), _ptr(dm),
+                                      _ptr(e))
     if code != _lib.MTP_OK:
         raise _lib.MTPError(code, "schedule emulation failed")
     return m, dm, float(e[0])

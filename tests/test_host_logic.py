@@ -75,15 +75,15 @@ def test_cpp_parser_rejects_bad_files(tmp_path):
         parse_info(str(f))
 
 
-@pytest.mark.parametrize("name,lanes", [("cfg0_L16_S1.mtp", 128), ("cfg0_L16_S1.mtp", 512),
-                                        ("cfg3_L20_S2.mtp", 256), ("cfg2_L24_S3.mtp", 256),
-                                        ("cfg4_L28_S4.mtp", 512)])
-def test_schedule_reproduces_tree_and_adjoint(name, lanes):
+@pytest.mark.parametrize("name,lanes,width", [("cfg0_L16_S1.mtp", 128, 4), ("cfg0_L16_S1.mtp", 512, 8),
+                                              ("cfg3_L20_S2.mtp", 256, 16), ("cfg2_L24_S3.mtp", 256, 4),
+                                              ("cfg2_L24_S3.mtp", 512, 8), ("cfg4_L28_S4.mtp", 512, 8)])
+def test_schedule_reproduces_tree_and_adjoint(name, lanes, width):
     pot = read_mtp(potential_path(name))
     tab = O.OracleTables.from_potential(pot)
     rng = np.random.default_rng(7)
     basic = rng.normal(size=pot.alpha_index_basic_count)
-    m, dm, e = schedule_emulate(potential_path(name), lanes, basic)
+    m, dm, e = schedule_emulate(potential_path(name), lanes, basic, width)
     # oracle: the same tree on the same basic moments, dE/dm by autograd
     b = torch.tensor(basic, requires_grad=True)
     mm = torch.cat([b, torch.zeros(tab.M - len(basic))])[None]

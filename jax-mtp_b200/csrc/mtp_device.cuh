@@ -76,7 +76,7 @@ struct DevIO {
 
 // Shared-memory carve of the evaluation kernel.
 // Lane-program entries requested ahead of use (registers), per thread.
-constexpr int kPrefetch = 8;
+constexpr int kPrefetch = kStepAlign;
 
 // Shared-memory carve of the evaluation kernel for A atoms per block: the
 // value space is interleaved [slot][atom] so one vector access serves all A
@@ -125,71 +125,94 @@ struct __align__(sizeof(T) * A) Pack {
   T v[A];
 };
 
+// Integer multiplicity of an entry (y & kMultMask < 2^14) as T without an
+// int-to-float conversion instruction: OR-ing m into the mantissa of 2^23
+// (2^52) gives the float (double) 2^23 + m exactly, and subtracting 2^23
+// (2^52) leaves m exactly.
+template <typename T>
+__device__ __forceinline__ T entry_mult(uint32_t y);
+template <>
+__device__ __forceinline__ float entry_mult<float>(uint32_t y) {
+  return __int_as_float(static_cast<int>((y & kMultMask) | 0x4B000000u)) - 8388608.0f;
+}
+template <>
+__device__ __forceinline__ double entry_mult<double>(uint32_t y) {
+  return __hiloint2double(0x43300000, static_cast<int>(y & kMultMask)) - 4503599627370496.0;
+}
+
 // Stream one lane program pass: every thread walks its column of the
-// [steps][lanes] entry array with kPrefetch entries in flight (registers), so
-// the L2 latency of the program overlaps the arithmetic.  Each entry feeds A
-// atoms: acc[a] += c * V[x][a] * V[y][a]; STORE/ADD flush into V[d][a].
-template <typename T, int A>
-__device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int steps, int lanes, int tid,
-                                         T* __restrict__ V) {
+// [steps][LANES] entry array with kPrefetch entries in flight (registers), so
+// the L2 latency of the program overlaps the arithmetic.  LANES is a template
+// argument so every request is one load at a constant offset; steps is a
+// multiple of kPrefetch and the program holds kPrefetch rows after any pass,
+// so nothing is bounds-tested.  Each entry feeds A atoms:
+// acc[a] += c * V[x][a] * V[y][a]; STORE/ADD flush into V[d][a].
+template <typename T, int A, int LANES>
+__device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int steps, int tid, T* __restrict__ V) {
+  static_assert(kPrefetch == kStepAlign, "prefetch depth must equal the pass step alignment");
   const uint2* p = ent + tid;
   uint2 buf[kPrefetch];
 #pragma unroll
-  for (int k = 0; k < kPrefetch; ++k) buf[k] = k < steps ? __ldg(p + static_cast<size_t>(k) * lanes) : make_uint2(0u, 0u);
+  for (int k = 0; k < kPrefetch; ++k) buf[k] = __ldg(p + k * LANES);
   T acc[A];
 #pragma unroll
   for (int a = 0; a < A; ++a) acc[a] = T(0);
   for (int s0 = 0; s0 < steps; s0 += kPrefetch) {
+    p += kPrefetch * LANES;
 #pragma unroll
     for (int k = 0; k < kPrefetch; ++k) {
-      if (s0 + k < steps) {
-        const uint2 e = buf[k];
-        const int nx = s0 + k + kPrefetch;
-        if (nx < steps) buf[k] = __ldg(p + static_cast<size_t>(nx) * lanes);
-        const T c = static_cast<T>(e.y >> 18);
-        const Pack<T, A> va = *reinterpret_cast<const Pack<T, A>*>(V + (e.x & 0xFFFFu) * A);
-        const Pack<T, A> vb = *reinterpret_cast<const Pack<T, A>*>(V + (e.x >> 16) * A);
+      const uint2 e = buf[k];
+      buf[k] = __ldg(p + k * LANES);
+      const T c = entry_mult<T>(e.y);
+      const Pack<T, A> va = *reinterpret_cast<const Pack<T, A>*>(V + (e.x & 0xFFFFu) * A);
+      const Pack<T, A> vb = *reinterpret_cast<const Pack<T, A>*>(V + (e.x >> 16) * A);
 #pragma unroll
-        for (int a = 0; a < A; ++a) acc[a] = dev_fma(c * va.v[a], vb.v[a], acc[a]);
-        const uint32_t op = (e.y >> 16) & 3u;
-        if (op) {
-          Pack<T, A>* dst = reinterpret_cast<Pack<T, A>*>(V + (e.y & 0xFFFFu) * A);
-          Pack<T, A> out;
-          if (op == kOpStore) {
+      for (int a = 0; a < A; ++a) acc[a] = dev_fma(c * va.v[a], vb.v[a], acc[a]);
+      if (e.y & (3u << kOpShift)) {
+        Pack<T, A>* dst = reinterpret_cast<Pack<T, A>*>(V + (e.y >> kDstShift) * A);
+        Pack<T, A> out;
+        if (e.y & (kOpStore << kOpShift)) {
 #pragma unroll
-            for (int a = 0; a < A; ++a) out.v[a] = acc[a];
-          } else {
-            out = *dst;
+          for (int a = 0; a < A; ++a) out.v[a] = acc[a];
+        } else {
+          out = *dst;
 #pragma unroll
-            for (int a = 0; a < A; ++a) out.v[a] += acc[a];
-          }
-          *dst = out;
-#pragma unroll
-          for (int a = 0; a < A; ++a) acc[a] = T(0);
+          for (int a = 0; a < A; ++a) out.v[a] += acc[a];
         }
+        *dst = out;
+#pragma unroll
+        for (int a = 0; a < A; ++a) acc[a] = T(0);
       }
     }
   }
 }
 
+// run_pass for the block's lane count (128, 256 or 512 threads).
+template <typename T, int A>
+__device__ __forceinline__ void run_pass_n(const uint2* __restrict__ ent, int steps, int lanes, int tid,
+                                           T* __restrict__ V) {
+  if (lanes == 512) run_pass<T, A, 512>(ent, steps, tid, V);
+  else if (lanes == 256) run_pass<T, A, 256>(ent, steps, tid, V);
+  else run_pass<T, A, 128>(ent, steps, tid, V);
+}
+
 // Generic lane-program streamer (used by the dual-number kernels): every thread
-// walks its column of the [steps][lanes] entries with kPrefetch in flight.
+// walks its column of the [steps][lanes] entries with kPrefetch in flight
+// (steps is a multiple of kPrefetch, rows after a pass exist).
 template <typename Body>
 __device__ __forceinline__ void stream_entries(const uint2* __restrict__ ent, int steps, int lanes, int tid,
                                                Body& body) {
   const uint2* p = ent + tid;
   uint2 buf[kPrefetch];
 #pragma unroll
-  for (int k = 0; k < kPrefetch; ++k) buf[k] = k < steps ? __ldg(p + static_cast<size_t>(k) * lanes) : make_uint2(0u, 0u);
+  for (int k = 0; k < kPrefetch; ++k) buf[k] = __ldg(p + static_cast<size_t>(k) * lanes);
   for (int s0 = 0; s0 < steps; s0 += kPrefetch) {
+    p += static_cast<size_t>(kPrefetch) * lanes;
 #pragma unroll
     for (int k = 0; k < kPrefetch; ++k) {
-      if (s0 + k < steps) {
-        const uint2 e = buf[k];
-        const int nx = s0 + k + kPrefetch;
-        if (nx < steps) buf[k] = __ldg(p + static_cast<size_t>(nx) * lanes);
-        body(e);
-      }
+      const uint2 e = buf[k];
+      buf[k] = __ldg(p + static_cast<size_t>(k) * lanes);
+      body(e);
     }
   }
 }
@@ -414,7 +437,7 @@ __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
 
     // ---- T: forward contraction passes ----------------------------------
     for (int ps = 0; ps < md.nfwd; ++ps) {
-      run_pass<T, A>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, V);
+      run_pass_n<T, A>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, V);
       __syncthreads();
     }
     // energy: E_i = xi[t_i] + sum_alpha theta_alpha m[map_alpha] in FP64
@@ -443,7 +466,7 @@ __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
 
     // ---- R: reverse passes (dE/dm) ---------------------------------------
     for (int ps = 0; ps < md.nrev; ++ps) {
-      run_pass<T, A>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, V);
+      run_pass_n<T, A>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, V);
       __syncthreads();
     }
 

@@ -557,26 +557,35 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
     if (v >= kSymPartBase) return static_cast<uint32_t>(s.v_part) + (v - kSymPartBase);
     return v;
   };
+  const uint32_t nop_x = static_cast<uint32_t>(s.v_zero) | (static_cast<uint32_t>(s.v_zero) << 16);
+  auto push_nops = [&](size_t n) {
+    for (size_t i = 0; i < n; ++i) {
+      s.entries.push_back(nop_x);
+      s.entries.push_back(0u);
+    }
+  };
   auto flush_passes = [&](std::vector<RawPass>& raw, std::vector<Pass>& dst) {
     for (RawPass& rp : raw) {
       Pass p;
       p.offset = static_cast<int>(s.entries.size() / 2);
-      p.steps = rp.steps;
+      p.steps = (rp.steps + kStepAlign - 1) / kStepAlign * kStepAlign;
       for (const RawEntry& r : rp.e) {
         uint32_t a = resolve(r.a), b = resolve(r.b), d = resolve(r.dst);
         s.entries.push_back(a | (b << 16));
-        s.entries.push_back(d | (r.op << 16) | (r.c << 18));
+        s.entries.push_back(r.c | (r.op << kOpShift) | (d << kDstShift));
       }
+      push_nops(static_cast<size_t>(p.steps - rp.steps) * lanes);
       dst.push_back(p);
     }
   };
   flush_passes(fwd, s.fwd);
   flush_passes(rev, s.rev);
+  push_nops(static_cast<size_t>(kStepAlign) * lanes);
   // every operand and destination must lie inside the value space
   for (size_t e = 0; e < s.entries.size(); e += 2) {
     const uint32_t x = s.entries[e], y = s.entries[e + 1];
     if ((x & 0xFFFFu) >= static_cast<uint32_t>(s.v_size) || (x >> 16) >= static_cast<uint32_t>(s.v_size) ||
-        (y & 0xFFFFu) >= static_cast<uint32_t>(s.v_size)) {
+        (y >> kDstShift) >= static_cast<uint32_t>(s.v_size)) {
       err = "internal error: schedule operand outside the value space";
       return false;
     }
@@ -603,8 +612,8 @@ double emulate_schedule(const Potential& pot, const Schedule& s, std::vector<dou
       for (int st = 0; st < p.steps; ++st) {
         size_t e = static_cast<size_t>(p.offset) + static_cast<size_t>(st) * s.lanes + l;
         uint32_t x = s.entries[2 * e], y = s.entries[2 * e + 1];
-        int a = x & 0xFFFF, b = x >> 16, d = y & 0xFFFF, op = (y >> 16) & 3;
-        double c = static_cast<double>(y >> 18);
+        int a = x & 0xFFFF, b = x >> 16, d = y >> kDstShift, op = (y >> kOpShift) & 3;
+        double c = static_cast<double>(y & kMultMask);
         acc = std::fma(c * V[a], V[b], acc);
         if (op != kOpNone) {
           writes.push_back({d, {static_cast<int>(op), acc}});

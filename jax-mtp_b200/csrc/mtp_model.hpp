@@ -13,7 +13,16 @@
 //     following combine pass.
 //
 // Every pass is a dense [steps][lanes] array of 8-byte entries so a warp
-// reads its entries with one coalesced 256-byte load per step.
+// reads its entries with one coalesced 256-byte load per step:
+//
+//   x = a | b << 16                     operand slots of the product
+//   y = mult | op << 14 | dst << 16     integer multiplicity (< 2^14), flush
+//                                       op (none/store/add), flush slot
+//
+// Steps are padded to a multiple of kStepAlign with no-op entries (operands
+// the constant-zero slot, y = 0), and kStepAlign no-op rows follow the last
+// pass, so a lane may request the kStepAlign rows after any step without a
+// bounds test.
 #pragma once
 
 #include <cstdint>
@@ -26,6 +35,7 @@ constexpr int kMaxR = 8;       // radial functions supported by the kernels
 constexpr int kMaxK = 16;      // Chebyshev terms supported by the kernels
 constexpr int kMaxDegree = 12; // monomial degree supported by the kernels
 constexpr int kMaxPasses = 16;
+constexpr int kStepAlign = 8;   // pass steps are a multiple of this; as many no-op rows end the program
 
 struct Potential {
   std::string version, potential_name, potential_tag, radial_basis_type;
@@ -45,10 +55,14 @@ bool parse_mtp_file(const std::string& path, Potential& out, std::string& err);
 
 // Program entry ops.
 enum : uint32_t { kOpNone = 0, kOpStore = 1, kOpAdd = 2 };
+// Fields of the second entry word.
+constexpr uint32_t kMultMask = 0x3FFFu;
+constexpr int kOpShift = 14;
+constexpr int kDstShift = 16;
 
 struct Pass {
   int offset = 0;   // first entry (index into Schedule::entries)
-  int steps = 0;    // entries per lane
+  int steps = 0;    // entries per lane (a multiple of kStepAlign)
 };
 
 struct Schedule {
@@ -69,7 +83,7 @@ struct Schedule {
   std::vector<int> mono_k;      // [P][kMaxR] basic-moment index for each mu or -1
   std::vector<int> zero_list;   // non-basic moments never written (must read as 0)
   std::vector<Pass> fwd, rev;   // passes in execution order
-  std::vector<uint32_t> entries;  // pairs (x, y) per entry: 2 words
+  std::vector<uint32_t> entries;  // pairs (x, y) per entry: 2 words; kStepAlign no-op rows at the end
   int max_depth = 0;
 };
 

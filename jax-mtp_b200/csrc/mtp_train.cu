@@ -52,14 +52,14 @@ struct DualFwdBody {
   int H;
   T acc, tac;
   __device__ __forceinline__ void operator()(const uint2 e) {
-    const T c = static_cast<T>(e.y >> 18);
+    const T c = entry_mult<T>(e.y);
     const uint32_t a = e.x & 0xFFFFu, b = e.x >> 16;
     const T va = V[a], vb = V[b], ta = V[a + H], tb = V[b + H];
     acc = dev_fma(c * va, vb, acc);
     tac = dev_fma(c, dev_fma(ta, vb, va * tb), tac);
-    const uint32_t op = (e.y >> 16) & 3u;
+    const uint32_t op = (e.y >> kOpShift) & 3u;
     if (op) {
-      const uint32_t d = e.y & 0xFFFFu;
+      const uint32_t d = e.y >> kDstShift;
       if (op == kOpStore) {
         V[d] = acc;
         V[d + H] = tac;
@@ -81,14 +81,14 @@ struct DualRevBody {
   int H;
   T acc, tac;
   __device__ __forceinline__ void operator()(const uint2 e) {
-    const T c = static_cast<T>(e.y >> 18);
+    const T c = entry_mult<T>(e.y);
     const uint32_t a = e.x & 0xFFFFu, b = e.x >> 16;
     const T la = V[a], ta = V[a + H], mb = V[b], tb = V[b + H];
     acc = dev_fma(c, dev_fma(la, mb, ta * tb), acc);
     tac = dev_fma(c * ta, mb, tac);
-    const uint32_t op = (e.y >> 16) & 3u;
+    const uint32_t op = (e.y >> kOpShift) & 3u;
     if (op) {
-      const uint32_t d = e.y & 0xFFFFu;
+      const uint32_t d = e.y >> kDstShift;
       if (op == kOpStore) {
         V[d] = acc;
         V[d + H] = tac;

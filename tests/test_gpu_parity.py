@@ -91,17 +91,43 @@ def test_deterministic_bitwise():
     assert np.array_equal(a["virial"], b["virial"])
 
 
-@pytest.mark.parametrize("threads", [128, 256, 512])
-def test_launch_shapes_agree(threads):
+SHAPES = [(128, 1), (256, 1), (512, 1), (256, 2), (512, 2), (256, 4), (512, 4)]
+
+
+@pytest.mark.parametrize("threads,apb", SHAPES)
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_launch_shapes_agree(threads, apb, precision):
+    """Every (threads, atoms per block) request gives the oracle's result.
+
+    Atom counts 32 and 13: with 13 atoms the last block holds fewer atoms than
+    atoms_per_block, so the empty-slot paths run next to real atoms."""
+    if precision == "fp64" and apb > 2:
+        pytest.skip("FP64 evaluates at most 2 atoms per block")
     g = golden_case("fcc32_L24")
     path = potential_path(str(g["potential"]))
-    ref = O.evaluate(read_mtp(path), g["itypes"], g["rijs"], g["js"], g["jtypes"], float(g["volume"]))
-    N, n = g["js"].shape
-    with MTPEngine(path, N, n) as eng:
-        eng.set_launch(threads)
-        out = eng.compute(g["itypes"], g["rijs"], g["js"], g["jtypes"], g["counts"])
-        assert eng.launch()["threads"] in (threads, 256, 128)
-    assert _rel(out["forces"], ref["forces"]) <= REL
+    pot = read_mtp(path)
+    for n_atoms in (32, 13):
+        it, rij = g["itypes"][:n_atoms], g["rijs"][:n_atoms]
+        js = np.where(g["js"][:n_atoms] < n_atoms, g["js"][:n_atoms], -1).astype(np.int32)
+        jt = np.where(js >= 0, g["jtypes"][:n_atoms], -1).astype(np.int32)   # drop neighbours outside the subset
+        ref = O.evaluate(pot, it, rij, js, jt, float(g["volume"]))
+        N, n = js.shape
+        with MTPEngine(path, N, n, precision=precision) as eng:
+            eng.set_launch(threads, 0, apb)
+            out = eng.compute(it, rij, js, jt, g["counts"][:n_atoms], eatom=True)
+            ran = eng.launch()
+        # a request that does not fit in shared memory falls back to the
+        # global-memory value space with one atom per block
+        assert ran["threads"] in (threads, 256, 128) and ran["atoms_per_block"] in (apb, 1)
+        if precision == "fp64":
+            assert _rel(out["site_energies"], ref["site_energies"]) <= REL
+            assert _rel(out["forces"], ref["forces"]) <= REL
+            assert _rel(out["virial"], ref["virial"]) <= REL
+        else:
+            fscale = max(1.0, np.abs(ref["forces"]).max())
+            escale = max(1.0, np.abs(ref["site_energies"]).max())
+            assert np.abs(out["site_energies"] - ref["site_energies"]).max() * 1e3 <= 0.1 * escale
+            assert np.abs(out["forces"] - ref["forces"]).max() * 1e3 <= 1.0 * fscale
 
 
 def test_edge_cases():

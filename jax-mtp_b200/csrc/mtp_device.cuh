@@ -54,8 +54,11 @@ struct DevModel {
   const int* zero_list;     // [nzero]
   const int* mono_abc;      // [P][4]
   const int* mono_k;        // [P][kMaxR]
+  const int* pair_base;     // [npairs] first dense slot of each (a, b) pair
+  const int* dense_k;       // [Q][kMaxR] basic moment of dense slot and mu, or -1
   int nseed, nzero;
   int S, R, K, M, B, P, D, Sa;
+  int Q, npairs;
   int v_m, v_dm, v_zero, v_one, v_size;
   double scaling, rmin, rmax;
 };
@@ -107,7 +110,7 @@ __host__ __device__ inline SmemLayout smem_layout(int v_size, int S, int R, int 
   L.slot = take(sizeof(int) * n_pad * A);
   L.abc = take(sizeof(int) * 4 * P);
   L.mk = take(sizeof(int) * kMaxR * P);
-  L.dmt = take(sizeof(T) * R * P * A);
+  L.dmt = take(sizeof(T) * R * ((D + 1) * (D + 2) * (D + 3) / 6) * A);   // dense simplex
   L.red = take(sizeof(double) * (threads / 32) * A);
   L.cnt = take(sizeof(int) * (threads / 32 + 1));
   L.total = (o + 31) & ~size_t(31);
@@ -217,6 +220,59 @@ __device__ __forceinline__ void stream_entries(const uint2* __restrict__ ent, in
   }
 }
 
+// Force-phase sums of one neighbour over this thread's share of the monomial
+// simplex.  With W_s = sum_mu Dm[s][mu] f_mu(d), W'_s the same with f'_mu,
+// and Q(u) = sum_s W_s u_x^a u_y^b u_z^c over slots s = (a, b, c):
+//   G = grad_u Q = (Gx, Gy, Gz),   S = sum_s W'_s u_x^a u_y^b u_z^c.
+// Each (a, b) pair is a Horner chain in u_z over c = D-a-b .. 0 (value and
+// z-derivative), scaled by the stored powers of u_x and u_y.  The tpn threads
+// of a neighbour take the pairs in snake order (sl, 2 tpn-1-sl, 2 tpn+sl, ...)
+// of the pair order (a + b ascending), so their shares differ by one pair at
+// most and run in step.
+template <typename T, int R>
+__device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, const int* __restrict__ pair_base, int D,
+                                        int npairs, int D1, const T* __restrict__ fq, const T* __restrict__ fpq,
+                                        const T* __restrict__ pw, T uz, int sl, int tpn, T& S, T& Gx, T& Gy, T& Gz) {
+  T f[R], fp[R];
+#pragma unroll
+  for (int mu = 0; mu < R; ++mu) {
+    f[mu] = fq[mu];
+    fp[mu] = fpq[mu];
+  }
+  int s = 0, sb = 0;   // diagonal a + b of the current pair and its first pair index
+  for (int k = 0;; ++k) {
+    const int i = (k >> 1) * 2 * tpn + ((k & 1) ? 2 * tpn - 1 - sl : sl);
+    if (i >= npairs) break;
+    while (i >= sb + s + 1) {
+      sb += s + 1;
+      ++s;
+    }
+    const int ea = i - sb, eb = s - ea, top = D - s;
+    const T* drow = dmt + (__ldg(pair_base + i) + top) * R;
+    T h = T(0), hz = T(0), hs = T(0);
+    for (int c = top; c >= 0; --c, drow -= R) {
+      T w = T(0), wp = T(0);
+#pragma unroll
+      for (int mu = 0; mu < R; ++mu) {
+        const T g = drow[mu];
+        w = dev_fma(g, f[mu], w);
+        wp = dev_fma(g, fp[mu], wp);
+      }
+      hz = dev_fma(hz, uz, h);
+      h = dev_fma(h, uz, w);
+      hs = dev_fma(hs, uz, wp);
+    }
+    const T xa = pw[ea], yb = pw[D1 + eb];
+    const T dxa = ea > 0 ? static_cast<T>(ea) * pw[ea - 1] : T(0);
+    const T dyb = eb > 0 ? static_cast<T>(eb) * pw[D1 + eb - 1] : T(0);
+    const T xy = xa * yb;
+    Gx = dev_fma(dxa * yb, h, Gx);
+    Gy = dev_fma(xa * dyb, h, Gy);
+    Gz = dev_fma(xy, hz, Gz);
+    S = dev_fma(xy, hs, S);
+  }
+}
+
 // Deterministic block sums of A doubles per thread (valid in thread 0).
 template <int A>
 __device__ __forceinline__ void block_sum(double (&v)[A], double* red) {
@@ -245,8 +301,16 @@ __device__ __forceinline__ void block_sum(double (&v)[A], double* red) {
 // space (moments, adjoints, partials) is a private slice of global memory
 // (L1/L2-resident) instead of shared memory; used when it does not fit in
 // shared memory (level 28 in FP64).
+// Register budget per thread: the FP32 one-atom variant runs three 256-thread
+// blocks per SM (80 registers fit 768 threads); the others run one block of
+// up to 512 threads.
 template <typename T, bool kVGlobal, int A>
-__global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
+struct EvalRegs {
+  static constexpr int value = (sizeof(T) == 4 && !kVGlobal && A == 1) ? 80 : 128;
+};
+
+template <typename T, bool kVGlobal, int A>
+__global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevModel md, DevIO io) {
   extern __shared__ __align__(32) unsigned char smem[];
   const int NT = blockDim.x;
   const int tid = threadIdx.x;
@@ -471,11 +535,13 @@ __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
     }
 
     // ---- N3: dE_i/dr_ij per kept neighbour -------------------------------
-    // dense table D[a][p][mu] = dE/dm of basic moment (mu, p) (0 if absent)
+    // dense table Dm[a][slot][mu] = dE/dm of basic moment (mu, slot) over the
+    // full monomial simplex in pair order (0 where the basis has no moment)
     T* sDm = reinterpret_cast<T*>(smem + L.dmt);
-    for (int x = tid; x < P * R * A; x += NT) {
-      const int a = x / (P * R), pm = x % (P * R);
-      const int k = sMk[kMaxR * (pm / R) + pm % R];
+    const int QR = md.Q * R;
+    for (int x = tid; x < QR * A; x += NT) {
+      const int a = x / QR, r = x - a * QR;
+      const int k = __ldg(md.dense_k + (r / R) * kMaxR + r % R);
       sDm[x] = k >= 0 ? V[(md.v_dm + k) * A + a] : T(0);
     }
     __syncthreads();
@@ -499,33 +565,20 @@ __global__ void __launch_bounds__(512) k_mtp_eval(DevModel md, DevIO io) {
         const int sl = idx & (tpn - 1);
         T Ssum = T(0), Gx = T(0), Gy = T(0), Gz = T(0);
         if (active) {
-          T f[kMaxR], fp[kMaxR];
-#pragma unroll
-          for (int mu = 0; mu < kMaxR; ++mu) {
-            f[mu] = mu < R ? sF[q * R + mu] : T(0);
-            fp[mu] = mu < R ? sFp[q * R + mu] : T(0);
-          }
+          const T* dmt = sDm + static_cast<size_t>(a) * QR;
+          const T* fq = sF + q * R;
+          const T* fpq = sFp + q * R;
           const T* pw = sPw + q * pws;
-          const T* dmt = sDm + static_cast<size_t>(a) * P * R;
-#pragma unroll 2
-          for (int p = sl; p < P; p += tpn) {
-            const int4 abc = *reinterpret_cast<const int4*>(sAbc + 4 * p);
-            const int ea = abc.x, eb = abc.y, ec = abc.z;
-            const T* drow = dmt + p * R;
-            T W = T(0), Wp = T(0);
-#pragma unroll
-            for (int mu = 0; mu < kMaxR; ++mu) {
-              if (mu < R) {
-                const T g = drow[mu];
-                W = dev_fma(g, f[mu], W);
-                Wp = dev_fma(g, fp[mu], Wp);
-              }
-            }
-            const T px = pw[ea], py = pw[D1 + eb], pz = pw[2 * D1 + ec];
-            Ssum = dev_fma(Wp, px * py * pz, Ssum);
-            Gx = dev_fma(W * static_cast<T>(ea), pw[ea > 0 ? ea - 1 : 0] * py * pz, Gx);
-            Gy = dev_fma(W * static_cast<T>(eb), px * pw[D1 + (eb > 0 ? eb - 1 : 0)] * pz, Gy);
-            Gz = dev_fma(W * static_cast<T>(ec), px * py * pw[2 * D1 + (ec > 0 ? ec - 1 : 0)], Gz);
+          const T uz = sU[4 * q + 2];
+          switch (R) {
+#define MTP_N3_CASE(RR)                                                                                 \
+  case RR:                                                                                              \
+    n3_sums<T, RR>(dmt, md.pair_base, md.D, md.npairs, D1, fq, fpq, pw, uz, sl, tpn, Ssum, Gx, Gy, Gz); \
+    break;
+            MTP_N3_CASE(1) MTP_N3_CASE(2) MTP_N3_CASE(3) MTP_N3_CASE(4)
+            MTP_N3_CASE(5) MTP_N3_CASE(6) MTP_N3_CASE(7) MTP_N3_CASE(8)
+#undef MTP_N3_CASE
+            default: break;
           }
         }
         for (int o = tpn >> 1; o > 0; o >>= 1) {

@@ -481,6 +481,26 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
     if (s.mono_k[kMaxR * p + mu] >= 0) { err = "duplicate row in alpha_index_basic"; return false; }
     s.mono_k[kMaxR * p + mu] = k;
   }
+  // dense simplex in pair order
+  s.npairs = (s.D + 1) * (s.D + 2) / 2;
+  s.Q = (s.D + 1) * (s.D + 2) * (s.D + 3) / 6;
+  s.pair_base.assign(s.npairs, 0);
+  s.dense_k.assign(static_cast<size_t>(s.Q) * kMaxR, -1);
+  {
+    int slot = 0, i = 0;
+    for (int sum = 0; sum <= s.D; ++sum) {
+      for (int a = 0; a <= sum; ++a, ++i) {
+        const int b = sum - a;
+        s.pair_base[i] = slot;
+        for (int c = 0; c <= s.D - sum; ++c, ++slot) {
+          auto it = mono_of.find(std::make_tuple(a, b, c));
+          if (it == mono_of.end()) continue;
+          for (int mu = 0; mu < kMaxR; ++mu)
+            s.dense_k[static_cast<size_t>(slot) * kMaxR + mu] = s.mono_k[kMaxR * it->second + mu];
+        }
+      }
+    }
+  }
   // moments that are read but never written stay zero for the whole run
   std::vector<char> read(M, 0);
   for (int e = 0; e < T; ++e) { read[pot.times[4 * e]] = 1; read[pot.times[4 * e + 1]] = 1; }

@@ -81,6 +81,13 @@ struct Schedule {
   int P = 0;              // distinct monomials
   std::vector<int> mono_abc;    // [P][4] (a, b, c, degree)
   std::vector<int> mono_k;      // [P][kMaxR] basic-moment index for each mu or -1
+  // The full monomial simplex a + b + c <= D in "pair order": pairs (a, b)
+  // by s = a + b ascending, then a ascending; each pair owns the run of
+  // slots c = 0 .. D - s.  Used by the force phase (nested Horner in z, y).
+  int Q = 0;                    // (D+1)(D+2)(D+3)/6 slots
+  int npairs = 0;               // (D+1)(D+2)/2 pairs
+  std::vector<int> pair_base;   // [npairs] first slot of each pair's run
+  std::vector<int> dense_k;     // [Q][kMaxR] basic-moment index of slot and mu, or -1
   std::vector<int> zero_list;   // non-basic moments never written (must read as 0)
   std::vector<Pass> fwd, rev;   // passes in execution order
   std::vector<uint32_t> entries;  // pairs (x, y) per entry: 2 words; kStepAlign no-op rows at the end

@@ -83,18 +83,24 @@ constexpr int kPrefetch = kStepAlign;
 
 // Shared-memory carve of the evaluation kernel for A atoms per block: the
 // value space is interleaved [slot][atom] so one vector access serves all A
-// atoms; neighbour staging is kept per atom.
+// atoms; neighbour staging is kept per atom.  The dense dE/dm table of the
+// force phase reuses the moment half of the value space (dead once the
+// reverse passes are done) when it fits there (Q R <= M); with the value
+// space in global memory, or when it does not fit, it gets its own region.
 struct SmemLayout {
   int pws;        // stride of a power row (3 (D+1), rounded up to odd)
-  size_t v, rad, u, f, fp, pw, slot, abc, mk, dmt, red, cnt, total;
+  bool dmt_in_v;  // dense table in the moment half of the value space
+  size_t v, rad, u, f, fp, pw, slot, dmt, red, cnt, total;
 };
 
 template <typename T>
-__host__ __device__ inline SmemLayout smem_layout(int v_size, int S, int R, int K, int P, int D, int n_pad,
+__host__ __device__ inline SmemLayout smem_layout(int v_size, int M, int S, int R, int K, int D, int n_pad,
                                                   int threads, int A) {
   SmemLayout L;
   L.pws = 3 * (D + 1);
   if ((L.pws & 1) == 0) L.pws += 1;
+  const int Q = (D + 1) * (D + 2) * (D + 3) / 6;
+  L.dmt_in_v = v_size > 0 && Q * R <= M;
   size_t o = 0;
   auto take = [&](size_t bytes) {
     size_t at = (o + 31) & ~size_t(31);
@@ -108,9 +114,7 @@ __host__ __device__ inline SmemLayout smem_layout(int v_size, int S, int R, int 
   L.fp = take(sizeof(T) * R * n_pad * A);
   L.pw = take(sizeof(T) * L.pws * n_pad * A);
   L.slot = take(sizeof(int) * n_pad * A);
-  L.abc = take(sizeof(int) * 4 * P);
-  L.mk = take(sizeof(int) * kMaxR * P);
-  L.dmt = take(sizeof(T) * R * ((D + 1) * (D + 2) * (D + 3) / 6) * A);   // dense simplex
+  L.dmt = L.dmt_in_v ? L.v : take(sizeof(T) * R * Q * A);
   L.red = take(sizeof(double) * (threads / 32) * A);
   L.cnt = take(sizeof(int) * (threads / 32 + 1));
   L.total = (o + 31) & ~size_t(31);
@@ -306,7 +310,7 @@ __device__ __forceinline__ void block_sum(double (&v)[A], double* red) {
 // up to 512 threads.
 template <typename T, bool kVGlobal, int A>
 struct EvalRegs {
-  static constexpr int value = (sizeof(T) == 4 && !kVGlobal && A == 1) ? 80 : 128;
+  static constexpr int value = (sizeof(T) == 4 && !kVGlobal && A == 1) ? 64 : 128;
 };
 
 template <typename T, bool kVGlobal, int A>
@@ -314,12 +318,10 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
   extern __shared__ __align__(32) unsigned char smem[];
   const int NT = blockDim.x;
   const int tid = threadIdx.x;
-  const SmemLayout L = smem_layout<T>(kVGlobal ? 0 : md.v_size, md.S, md.R, md.K, md.P, md.D, io.n_pad, NT, A);
+  const SmemLayout L = smem_layout<T>(kVGlobal ? 0 : md.v_size, md.M, md.S, md.R, md.K, md.D, io.n_pad, NT, A);
   T* V = kVGlobal ? reinterpret_cast<T*>(io.vscratch) + static_cast<size_t>(blockIdx.x) * md.v_size * A
                   : reinterpret_cast<T*>(smem + L.v);
   T* sRad = reinterpret_cast<T*>(smem + L.rad);
-  int* sAbc = reinterpret_cast<int*>(smem + L.abc);
-  int* sMk = reinterpret_cast<int*>(smem + L.mk);
   double* sRed = reinterpret_cast<double*>(smem + L.red);
   int* sCnt = reinterpret_cast<int*>(smem + L.cnt);
   const int n_pad = io.n_pad;
@@ -327,9 +329,6 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
   const int S = md.S, R = md.R, K = md.K, P = md.P, D1 = md.D + 1, pws = L.pws;
   // per-block constants
   for (int x = tid; x < S * S * R * K; x += NT) sRad[x] = static_cast<T>(md.radial[x]);
-  for (int x = tid; x < 4 * P; x += NT) sAbc[x] = md.mono_abc[x];
-  for (int x = tid; x < kMaxR * P; x += NT) sMk[x] = md.mono_k[x];
-  for (int x = tid; x < md.nzero * A; x += NT) V[(md.v_m + md.zero_list[x / A]) * A + x % A] = T(0);
   for (int a = tid; a < A; a += NT) {
     V[md.v_zero * A + a] = T(0);
     V[md.v_one * A + a] = T(1);
@@ -341,6 +340,9 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
   __syncthreads();
 
   for (int base = blockIdx.x * A; base < io.natoms; base += gridDim.x * A) {
+    // moments that are read but never written (the force phase of the
+    // previous atom may have reused their slots for its dense table)
+    for (int x = tid; x < md.nzero * A; x += NT) V[(md.v_m + md.zero_list[x / A]) * A + x % A] = T(0);
     int it_a[A], nv_a[A];
     // ---- N1 + N2 per atom of the group -------------------------------------
 #pragma unroll
@@ -471,7 +473,8 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
 
       // basic moments m[(mu, a, b, c)] of this atom into value lane a
       for (int p = tid; p < P; p += NT) {
-        const int ea = sAbc[4 * p], eb = sAbc[4 * p + 1], ec = sAbc[4 * p + 2];
+        const int4 abc = __ldg(reinterpret_cast<const int4*>(md.mono_abc) + p);
+        const int ea = abc.x, eb = abc.y, ec = abc.z;
         T acc[kMaxR];
 #pragma unroll
         for (int mu = 0; mu < kMaxR; ++mu) acc[mu] = T(0);
@@ -487,7 +490,7 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
 #pragma unroll
         for (int mu = 0; mu < kMaxR; ++mu) {
           if (mu < R) {
-            const int k = sMk[kMaxR * p + mu];
+            const int k = __ldg(md.mono_k + kMaxR * p + mu);
             if (k >= 0) V[(md.v_m + k) * A + a] = acc[mu];
           }
         }
@@ -537,7 +540,7 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
     // ---- N3: dE_i/dr_ij per kept neighbour -------------------------------
     // dense table Dm[a][slot][mu] = dE/dm of basic moment (mu, slot) over the
     // full monomial simplex in pair order (0 where the basis has no moment)
-    T* sDm = reinterpret_cast<T*>(smem + L.dmt);
+    T* sDm = L.dmt_in_v ? V + md.v_m * A : reinterpret_cast<T*>(smem + L.dmt);
     const int QR = md.Q * R;
     for (int x = tid; x < QR * A; x += NT) {
       const int a = x / QR, r = x - a * QR;

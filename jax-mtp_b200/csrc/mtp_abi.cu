@@ -132,6 +132,7 @@ DevModel make_model(mtp_handle* h, const DeviceSchedule& ds) {
   md.dense_k = h->d_dense_k;
   md.Q = s.Q;
   md.npairs = s.npairs;
+  for (int v = 0; v <= s.D; ++v) md.nmu[v] = s.nmu[v];
   md.S = h->pot.S;
   md.R = h->pot.R;
   md.K = h->pot.K;

@@ -59,6 +59,7 @@ struct DevModel {
   int nseed, nzero;
   int S, R, K, M, B, P, D, Sa;
   int Q, npairs;
+  int nmu[kMaxDegree + 1];  // radial functions with a basic moment of each degree
   int v_m, v_dm, v_zero, v_one, v_size;
   double scaling, rmin, rmax;
 };
@@ -277,6 +278,21 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, const int* __
   }
 }
 
+// Basic moments of one (atom, monomial) task for NM radial functions:
+// acc[mu] = sum_q f_mu(d_q) u_x^a u_y^b u_z^c over the kept neighbours.
+template <typename T, int NM>
+__device__ __forceinline__ void moment_task(const T* __restrict__ sF, const T* __restrict__ sPw, int R, int pws, int D1,
+                                            int nv, int ea, int eb, int ec, T (&acc)[kMaxR]) {
+#pragma unroll 4
+  for (int q = 0; q < nv; ++q) {
+    const T* pw = sPw + q * pws;
+    const T mono = pw[ea] * pw[D1 + eb] * pw[2 * D1 + ec];
+    const T* f = sF + q * R;
+#pragma unroll
+    for (int mu = 0; mu < NM; ++mu) acc[mu] = dev_fma(f[mu], mono, acc[mu]);
+  }
+}
+
 // Deterministic block sums of A doubles per thread (valid in thread 0).
 template <int A>
 __device__ __forceinline__ void block_sum(double (&v)[A], double* red) {
@@ -471,25 +487,40 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
       }
       nv_a[a] = nv;
 
-      // basic moments m[(mu, a, b, c)] of this atom into value lane a
-      for (int p = tid; p < P; p += NT) {
-        const int4 abc = __ldg(reinterpret_cast<const int4*>(md.mono_abc) + p);
-        const int ea = abc.x, eb = abc.y, ec = abc.z;
-        T acc[kMaxR];
+    }
+    // ---- N2: basic moments m[(mu, a, b, c)] of every atom of the block ------
+    // tasks (atom, monomial); monomials are sorted by degree, so the tasks of a
+    // warp share one radial-function count (the warp's largest is used)
+    for (int t0 = 0; t0 < A * P; t0 += NT) {
+      const int t = t0 + tid;
+      const bool act = t < A * P;
+      const int a = act ? t / P : 0, p = act ? t - a * P : 0;
+      const int4 abc = __ldg(reinterpret_cast<const int4*>(md.mono_abc) + p);
+      int nv = 0;
 #pragma unroll
-        for (int mu = 0; mu < kMaxR; ++mu) acc[mu] = T(0);
-#pragma unroll 4
-        for (int q = 0; q < nv; ++q) {
-          const T* pw = sPw + q * pws;
-          const T mono = pw[ea] * pw[D1 + eb] * pw[2 * D1 + ec];
-          const T* f = sF + q * R;
+      for (int aa = 0; aa < A; ++aa)
+        if (act && aa == a) nv = nv_a[aa];
+      const int nm = __reduce_max_sync(0xffffffffu, act ? md.nmu[abc.w] : 0);
+      const T* sF = reinterpret_cast<const T*>(smem + L.f) + static_cast<size_t>(a) * R * n_pad;
+      const T* sPw = reinterpret_cast<const T*>(smem + L.pw) + static_cast<size_t>(a) * pws * n_pad;
+      T acc[kMaxR];
 #pragma unroll
-          for (int mu = 0; mu < kMaxR; ++mu)
-            if (mu < R) acc[mu] = dev_fma(f[mu], mono, acc[mu]);
-        }
+      for (int mu = 0; mu < kMaxR; ++mu) acc[mu] = T(0);
+      switch (nm) {
+        case 0: break;
+        case 1: moment_task<T, 1>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 2: moment_task<T, 2>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 3: moment_task<T, 3>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 4: moment_task<T, 4>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 5: moment_task<T, 5>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 6: moment_task<T, 6>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 7: moment_task<T, 7>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        default: moment_task<T, 8>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+      }
+      if (act) {
 #pragma unroll
         for (int mu = 0; mu < kMaxR; ++mu) {
-          if (mu < R) {
+          if (mu < nm) {
             const int k = __ldg(md.mono_k + kMaxR * p + mu);
             if (k >= 0) V[(md.v_m + k) * A + a] = acc[mu];
           }

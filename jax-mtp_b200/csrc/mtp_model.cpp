@@ -462,6 +462,13 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
       monos.push_back(key);
     }
   }
+  // degree descending (then a, b, c): the threads of a warp in the basic-moment
+  // phase then hold monomials of one degree, i.e. one radial-function count
+  std::sort(monos.begin(), monos.end(), [](const std::tuple<int, int, int>& x, const std::tuple<int, int, int>& y) {
+    const int dx = std::get<0>(x) + std::get<1>(x) + std::get<2>(x), dy = std::get<0>(y) + std::get<1>(y) + std::get<2>(y);
+    return dx != dy ? dx > dy : x < y;
+  });
+  for (size_t p = 0; p < monos.size(); ++p) mono_of[monos[p]] = static_cast<int>(p);
   s.P = static_cast<int>(monos.size());
   s.mono_abc.assign(4 * s.P, 0);
   s.mono_k.assign(kMaxR * s.P, -1);
@@ -480,6 +487,13 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
     int p = mono_of[std::make_tuple(pot.basic[4 * k + 1], pot.basic[4 * k + 2], pot.basic[4 * k + 3])];
     if (s.mono_k[kMaxR * p + mu] >= 0) { err = "duplicate row in alpha_index_basic"; return false; }
     s.mono_k[kMaxR * p + mu] = k;
+  }
+  // radial functions per degree: nmu[v] = 1 + the largest mu of a basic
+  // moment of degree v (0 if none)
+  s.nmu.assign(s.D + 1, 0);
+  for (int k = 0; k < B; ++k) {
+    const int v = pot.basic[4 * k + 1] + pot.basic[4 * k + 2] + pot.basic[4 * k + 3];
+    s.nmu[v] = std::max(s.nmu[v], pot.basic[4 * k] + 1);
   }
   // dense simplex in pair order
   s.npairs = (s.D + 1) * (s.D + 2) / 2;

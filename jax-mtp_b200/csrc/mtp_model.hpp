@@ -79,7 +79,8 @@ struct Schedule {
   // monomials of the basic moments
   int D = 0;              // max degree
   int P = 0;              // distinct monomials
-  std::vector<int> mono_abc;    // [P][4] (a, b, c, degree)
+  std::vector<int> mono_abc;    // [P][4] (a, b, c, degree), degree descending
+  std::vector<int> nmu;         // [D + 1] radial functions with a basic moment of each degree
   std::vector<int> mono_k;      // [P][kMaxR] basic-moment index for each mu or -1
   // The full monomial simplex a + b + c <= D in "pair order": pairs (a, b)
   // by s = a + b ascending, then a ascending; each pair owns the run of

@@ -255,17 +255,24 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, const int* __
     const int ea = i - sb, eb = s - ea, top = D - s;
     const T* drow = dmt + (__ldg(pair_base + i) + top) * R;
     T h = T(0), hz = T(0), hs = T(0);
+#pragma unroll 2
     for (int c = top; c >= 0; --c, drow -= R) {
-      T w = T(0), wp = T(0);
+      // two partial sums (even, odd mu) halve the dependent-FMA chain
+      T w0 = T(0), w1 = T(0), wp0 = T(0), wp1 = T(0);
 #pragma unroll
-      for (int mu = 0; mu < R; ++mu) {
+      for (int mu = 0; mu < R; mu += 2) {
         const T g = drow[mu];
-        w = dev_fma(g, f[mu], w);
-        wp = dev_fma(g, fp[mu], wp);
+        w0 = dev_fma(g, f[mu], w0);
+        wp0 = dev_fma(g, fp[mu], wp0);
+        if (mu + 1 < R) {
+          const T g1 = drow[mu + 1];
+          w1 = dev_fma(g1, f[mu + 1], w1);
+          wp1 = dev_fma(g1, fp[mu + 1], wp1);
+        }
       }
       hz = dev_fma(hz, uz, h);
-      h = dev_fma(h, uz, w);
-      hs = dev_fma(hs, uz, wp);
+      h = dev_fma(h, uz, w0 + w1);
+      hs = dev_fma(hs, uz, wp0 + wp1);
     }
     const T xa = pw[ea], yb = pw[D1 + eb];
     const T dxa = ea > 0 ? static_cast<T>(ea) * pw[ea - 1] : T(0);

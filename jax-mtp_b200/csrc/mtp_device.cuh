@@ -225,24 +225,29 @@ __device__ __forceinline__ void stream_entries(const uint2* __restrict__ ent, in
   }
 }
 
-// Force-phase sums of one neighbour over this thread's share of the monomial
-// simplex.  With W_s = sum_mu Dm[s][mu] f_mu(d), W'_s the same with f'_mu,
-// and Q(u) = sum_s W_s u_x^a u_y^b u_z^c over slots s = (a, b, c):
+// Force-phase sums of two neighbours over this thread's share of the
+// monomial simplex.  With W_s = sum_mu Dm[s][mu] f_mu(d), W'_s the same with
+// f'_mu, and Q(u) = sum_s W_s u_x^a u_y^b u_z^c over slots s = (a, b, c):
 //   G = grad_u Q = (Gx, Gy, Gz),   S = sum_s W'_s u_x^a u_y^b u_z^c.
 // Each (a, b) pair is a Horner chain in u_z over c = D-a-b .. 0 (value and
-// z-derivative), scaled by the stored powers of u_x and u_y.  The tpn threads
-// of a neighbour take the pairs in snake order (sl, 2 tpn-1-sl, 2 tpn+sl, ...)
-// of the pair order (a + b ascending), so their shares differ by one pair at
-// most and run in step.
+// z-derivative), scaled by the stored powers of u_x and u_y.  The dE/dm rows
+// are per atom, so the two neighbours share every row load and their chains
+// run side by side.  The tpn threads of a neighbour pair take the (a, b)
+// pairs in snake order (sl, 2 tpn-1-sl, 2 tpn+sl, ...) of the pair order
+// (a + b ascending), so their shares differ by one pair at most.
 template <typename T, int R>
 __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, const int* __restrict__ pair_base, int D,
-                                        int npairs, int D1, const T* __restrict__ fq, const T* __restrict__ fpq,
-                                        const T* __restrict__ pw, T uz, int sl, int tpn, T& S, T& Gx, T& Gy, T& Gz) {
-  T f[R], fp[R];
+                                        int npairs, int D1, const T* __restrict__ fq0, const T* __restrict__ fpq0,
+                                        const T* __restrict__ fq1, const T* __restrict__ fpq1, bool two,
+                                        const T* __restrict__ pw0, const T* __restrict__ pw1, T uz0, T uz1, int sl,
+                                        int tpn, T (&S)[2], T (&Gx)[2], T (&Gy)[2], T (&Gz)[2]) {
+  T f0[R], fp0[R], f1[R], fp1[R];
 #pragma unroll
   for (int mu = 0; mu < R; ++mu) {
-    f[mu] = fq[mu];
-    fp[mu] = fpq[mu];
+    f0[mu] = fq0[mu];
+    fp0[mu] = fpq0[mu];
+    f1[mu] = two ? fq1[mu] : T(0);
+    fp1[mu] = two ? fpq1[mu] : T(0);
   }
   int s = 0, sb = 0;   // diagonal a + b of the current pair and its first pair index
   for (int k = 0;; ++k) {
@@ -254,34 +259,45 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, const int* __
     }
     const int ea = i - sb, eb = s - ea, top = D - s;
     const T* drow = dmt + (__ldg(pair_base + i) + top) * R;
-    T h = T(0), hz = T(0), hs = T(0);
+    T h0 = T(0), hz0 = T(0), hs0 = T(0), h1 = T(0), hz1 = T(0), hs1 = T(0);
 #pragma unroll 2
     for (int c = top; c >= 0; --c, drow -= R) {
-      // two partial sums (even, odd mu) halve the dependent-FMA chain
-      T w0 = T(0), w1 = T(0), wp0 = T(0), wp1 = T(0);
+      T w0 = T(0), wp0 = T(0), w1 = T(0), wp1 = T(0);
 #pragma unroll
-      for (int mu = 0; mu < R; mu += 2) {
+      for (int mu = 0; mu < R; ++mu) {
         const T g = drow[mu];
-        w0 = dev_fma(g, f[mu], w0);
-        wp0 = dev_fma(g, fp[mu], wp0);
-        if (mu + 1 < R) {
-          const T g1 = drow[mu + 1];
-          w1 = dev_fma(g1, f[mu + 1], w1);
-          wp1 = dev_fma(g1, fp[mu + 1], wp1);
-        }
+        w0 = dev_fma(g, f0[mu], w0);
+        wp0 = dev_fma(g, fp0[mu], wp0);
+        w1 = dev_fma(g, f1[mu], w1);
+        wp1 = dev_fma(g, fp1[mu], wp1);
       }
-      hz = dev_fma(hz, uz, h);
-      h = dev_fma(h, uz, w0 + w1);
-      hs = dev_fma(hs, uz, wp0 + wp1);
+      hz0 = dev_fma(hz0, uz0, h0);
+      h0 = dev_fma(h0, uz0, w0);
+      hs0 = dev_fma(hs0, uz0, wp0);
+      hz1 = dev_fma(hz1, uz1, h1);
+      h1 = dev_fma(h1, uz1, w1);
+      hs1 = dev_fma(hs1, uz1, wp1);
     }
-    const T xa = pw[ea], yb = pw[D1 + eb];
-    const T dxa = ea > 0 ? static_cast<T>(ea) * pw[ea - 1] : T(0);
-    const T dyb = eb > 0 ? static_cast<T>(eb) * pw[D1 + eb - 1] : T(0);
-    const T xy = xa * yb;
-    Gx = dev_fma(dxa * yb, h, Gx);
-    Gy = dev_fma(xa * dyb, h, Gy);
-    Gz = dev_fma(xy, hz, Gz);
-    S = dev_fma(xy, hs, S);
+    {
+      const T xa = pw0[ea], yb = pw0[D1 + eb];
+      const T dxa = ea > 0 ? static_cast<T>(ea) * pw0[ea - 1] : T(0);
+      const T dyb = eb > 0 ? static_cast<T>(eb) * pw0[D1 + eb - 1] : T(0);
+      const T xy = xa * yb;
+      Gx[0] = dev_fma(dxa * yb, h0, Gx[0]);
+      Gy[0] = dev_fma(xa * dyb, h0, Gy[0]);
+      Gz[0] = dev_fma(xy, hz0, Gz[0]);
+      S[0] = dev_fma(xy, hs0, S[0]);
+    }
+    {
+      const T xa = pw1[ea], yb = pw1[D1 + eb];
+      const T dxa = ea > 0 ? static_cast<T>(ea) * pw1[ea - 1] : T(0);
+      const T dyb = eb > 0 ? static_cast<T>(eb) * pw1[D1 + eb - 1] : T(0);
+      const T xy = xa * yb;
+      Gx[1] = dev_fma(dxa * yb, h1, Gx[1]);
+      Gy[1] = dev_fma(xa * dyb, h1, Gy[1]);
+      Gz[1] = dev_fma(xy, hz1, Gz[1]);
+      S[1] = dev_fma(xy, hs1, S[1]);
+    }
   }
 }
 
@@ -596,25 +612,27 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
       const T* sPw = reinterpret_cast<T*>(smem + L.pw) + static_cast<size_t>(a) * pws * n_pad;
       const int* sSlot = reinterpret_cast<int*>(smem + L.slot) + a * n_pad;
       double* grow = io.pair_grad + static_cast<size_t>(atom < io.natoms ? atom : 0) * io.nbr_stride * 3;
+      // threads take pairs of neighbours (q, q + nt)
+      const int nt = (nv + 1) >> 1;
       int tpn = 32;
-      while (tpn > 1 && tpn * nv > NT) tpn >>= 1;
-      const int total = nv * tpn;
+      while (tpn > 1 && tpn * nt > NT) tpn >>= 1;
+      const int total = nt * tpn;
       for (int b0 = 0; b0 < total; b0 += NT) {
         const int idx = b0 + tid;
         const bool active = idx < total;
-        const int q = active ? idx / tpn : 0;
+        const int q0 = active ? idx / tpn : 0;
+        const int q1 = q0 + nt;
+        const bool two = active && q1 < nv;
         const int sl = idx & (tpn - 1);
-        T Ssum = T(0), Gx = T(0), Gy = T(0), Gz = T(0);
+        T Ssum[2] = {T(0), T(0)}, Gx[2] = {T(0), T(0)}, Gy[2] = {T(0), T(0)}, Gz[2] = {T(0), T(0)};
         if (active) {
           const T* dmt = sDm + static_cast<size_t>(a) * QR;
-          const T* fq = sF + q * R;
-          const T* fpq = sFp + q * R;
-          const T* pw = sPw + q * pws;
-          const T uz = sU[4 * q + 2];
+          const int qb = two ? q1 : q0;
           switch (R) {
-#define MTP_N3_CASE(RR)                                                                                 \
-  case RR:                                                                                              \
-    n3_sums<T, RR>(dmt, md.pair_base, md.D, md.npairs, D1, fq, fpq, pw, uz, sl, tpn, Ssum, Gx, Gy, Gz); \
+#define MTP_N3_CASE(RR)                                                                                        \
+  case RR:                                                                                                     \
+    n3_sums<T, RR>(dmt, md.pair_base, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R, sFp + qb * R, \
+                   two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2], sU[4 * qb + 2], sl, tpn, Ssum, Gx, Gy, Gz); \
     break;
             MTP_N3_CASE(1) MTP_N3_CASE(2) MTP_N3_CASE(3) MTP_N3_CASE(4)
             MTP_N3_CASE(5) MTP_N3_CASE(6) MTP_N3_CASE(7) MTP_N3_CASE(8)
@@ -622,26 +640,33 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
             default: break;
           }
         }
-        for (int o = tpn >> 1; o > 0; o >>= 1) {
-          Ssum += __shfl_xor_sync(0xffffffffu, Ssum, o);
-          Gx += __shfl_xor_sync(0xffffffffu, Gx, o);
-          Gy += __shfl_xor_sync(0xffffffffu, Gy, o);
-          Gz += __shfl_xor_sync(0xffffffffu, Gz, o);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          for (int o = tpn >> 1; o > 0; o >>= 1) {
+            Ssum[j] += __shfl_xor_sync(0xffffffffu, Ssum[j], o);
+            Gx[j] += __shfl_xor_sync(0xffffffffu, Gx[j], o);
+            Gy[j] += __shfl_xor_sync(0xffffffffu, Gy[j], o);
+            Gz[j] += __shfl_xor_sync(0xffffffffu, Gz[j], o);
+          }
         }
-        if (active && sl == 0) {
-          const T ux = sU[4 * q], uy = sU[4 * q + 1], uz = sU[4 * q + 2], d = sU[4 * q + 3];
-          const T ug = ux * Gx + uy * Gy + uz * Gz;
-          const T inv_d = T(1) / d;
-          const T gx = ux * Ssum + (Gx - ux * ug) * inv_d;
-          const T gy = uy * Ssum + (Gy - uy * ug) * inv_d;
-          const T gz = uz * Ssum + (Gz - uz * ug) * inv_d;
-          const int s = sSlot[q];
-          grow[3 * s] = static_cast<double>(gx);
-          grow[3 * s + 1] = static_cast<double>(gy);
-          grow[3 * s + 2] = static_cast<double>(gz);
-          if (!(isfinite(static_cast<double>(gx)) && isfinite(static_cast<double>(gy)) &&
-                isfinite(static_cast<double>(gz))))
-            atomicOr(io.err, kErrNonFinite);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int q = j ? q1 : q0;
+          if (active && sl == 0 && (j == 0 || two)) {
+            const T ux = sU[4 * q], uy = sU[4 * q + 1], uz = sU[4 * q + 2], d = sU[4 * q + 3];
+            const T ug = ux * Gx[j] + uy * Gy[j] + uz * Gz[j];
+            const T inv_d = T(1) / d;
+            const T gx = ux * Ssum[j] + (Gx[j] - ux * ug) * inv_d;
+            const T gy = uy * Ssum[j] + (Gy[j] - uy * ug) * inv_d;
+            const T gz = uz * Ssum[j] + (Gz[j] - uz * ug) * inv_d;
+            const int s = sSlot[q];
+            grow[3 * s] = static_cast<double>(gx);
+            grow[3 * s + 1] = static_cast<double>(gy);
+            grow[3 * s + 2] = static_cast<double>(gz);
+            if (!(isfinite(static_cast<double>(gx)) && isfinite(static_cast<double>(gy)) &&
+                  isfinite(static_cast<double>(gz))))
+              atomicOr(io.err, kErrNonFinite);
+          }
         }
       }
     }

@@ -84,6 +84,10 @@ struct mtp_handle {
   // profiling of the evaluation kernel
   bool profiling = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+  // host-buffer calls (mtp_compute) on large systems copy the inputs in atom
+  // chunks on copy_stream while the evaluation kernel runs on earlier chunks
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> chunk_events;
   int prof_used = 0;
   // statistics
   long long calls = 0;
@@ -225,6 +229,8 @@ void free_handle(mtp_handle* h) {
   }
   if (h->h_tot) cudaFreeHost(h->h_tot);
   if (h->h_err) cudaFreeHost(h->h_err);
+  for (auto ev : h->chunk_events) cudaEventDestroy(ev);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
@@ -312,49 +318,120 @@ int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, 
   return MTP_OK;
 }
 
-// Evaluate site energies and per-slot gradients, then forces and virials.
-int run_device(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
-               const int* jtypes, const int* counts, bool rebuild_incoming, double* forces, double* vatom) {
+// Evaluation kernel on atoms [lo, lo + n) of device rows (site energies and
+// per-slot gradients of those atoms).
+int eval_range(mtp_handle* h, int lo, int n, int stride, const int* itypes, const double* rijs, const int* jtypes,
+               const int* counts) {
   const bool fp64 = h->precision == MTP_PRECISION_FP64;
   DeviceSchedule* ds = nullptr;
   int blocks = 0;
   bool vglobal = false;
-  int st = pick_launch(h, natoms, stride, &ds, &blocks, fp64, &vglobal);
+  int st = pick_launch(h, n, stride, &ds, &blocks, fp64, &vglobal);
   if (st != MTP_OK) return st;
   DevModel md = make_model(h, *ds);
+  const size_t rows = static_cast<size_t>(lo) * stride;
   DevIO io{};
-  io.natoms = natoms;
+  io.natoms = n;
   io.nbr_stride = stride;
   io.n_pad = stride;
-  io.itypes = itypes;
-  io.rijs = rijs;
-  io.jtypes = jtypes;
-  io.counts = counts;
-  io.site_energy = h->d_E;
-  io.pair_grad = h->d_G;
+  io.itypes = itypes + lo;
+  io.rijs = rijs + 3 * rows;
+  io.jtypes = jtypes + rows;
+  io.counts = counts ? counts + lo : nullptr;
+  io.site_energy = h->d_E + lo;
+  io.pair_grad = h->d_G + 3 * rows;
   io.err = h->d_err;
   io.vscratch = h->d_vscratch;
+  MTP_CUDA(h, launch_eval(md, io, h->last_threads, blocks, fp64, vglobal, h->last_apb, h->stream));
+  return MTP_OK;
+}
+
+// Profiling events around the evaluation launches of one call (mtp_profile).
+int prof_begin(mtp_handle* h, cudaEvent_t* e1) {
+  *e1 = nullptr;
+  if (!h->profiling) return MTP_OK;
+  if (h->prof_used == static_cast<int>(h->prof_events.size())) {
+    cudaEvent_t a, b;
+    MTP_CUDA(h, cudaEventCreate(&a));
+    MTP_CUDA(h, cudaEventCreate(&b));
+    h->prof_events.push_back({a, b});
+  }
+  const cudaEvent_t e0 = h->prof_events[h->prof_used].first;
+  *e1 = h->prof_events[h->prof_used].second;
+  ++h->prof_used;
+  MTP_CUDA(h, cudaEventRecord(e0, h->stream));
+  return MTP_OK;
+}
+
+// Evaluate site energies and per-slot gradients, then forces and virials.
+int run_device(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
+               const int* jtypes, const int* counts, bool rebuild_incoming, double* forces, double* vatom) {
   if (rebuild_incoming) {
     MTP_CUDA(h, launch_incoming(natoms, stride, js, jtypes, counts, h->d_in_cnt, h->d_in_ptr, h->d_in_cursor,
                                 h->d_in_slot, h->d_blk, h->stream));
   }
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (h->profiling) {
-    if (h->prof_used == static_cast<int>(h->prof_events.size())) {
-      cudaEvent_t a, b;
-      MTP_CUDA(h, cudaEventCreate(&a));
-      MTP_CUDA(h, cudaEventCreate(&b));
-      h->prof_events.push_back({a, b});
-    }
-    e0 = h->prof_events[h->prof_used].first;
-    e1 = h->prof_events[h->prof_used].second;
-    ++h->prof_used;
-    MTP_CUDA(h, cudaEventRecord(e0, h->stream));
-  }
-  MTP_CUDA(h, launch_eval(md, io, h->last_threads, blocks, fp64, vglobal, h->last_apb, h->stream));
+  cudaEvent_t e1 = nullptr;
+  int st = prof_begin(h, &e1);
+  if (st != MTP_OK) return st;
+  st = eval_range(h, 0, natoms, stride, itypes, rijs, jtypes, counts);
+  if (st != MTP_OK) return st;
   if (e1) MTP_CUDA(h, cudaEventRecord(e1, h->stream));
   MTP_CUDA(h, launch_force_gather(natoms, stride, rijs, counts, h->d_G, h->d_in_ptr, h->d_in_slot, forces,
                                   h->d_wown, vatom, h->stream));
+  return MTP_OK;
+}
+
+// Systems from this size on are copied in chunks that overlap the evaluation.
+constexpr int kPipelineMinAtoms = 65536;
+constexpr int kPipelineChunks = 8;
+
+// run_device for host input buffers: the inputs of chunk k go up on the copy
+// stream while the evaluation kernel works on chunk k-1 (events order each
+// chunk's kernel after its copies); the incoming lists and the force gather
+// need every row and follow the last chunk.  With pinned host buffers the
+// copies overlap the kernels; pageable ones are still correct.
+int run_host_pipelined(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
+                       const int* jtypes, const int* counts, double* vatom) {
+  const cudaStream_t s = h->stream;
+  if (!h->copy_stream) MTP_CUDA(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+  const int nch = std::max(1, std::min(kPipelineChunks, natoms / (kPipelineMinAtoms / 2)));
+  while (static_cast<int>(h->chunk_events.size()) < nch + 1) {
+    cudaEvent_t ev;
+    MTP_CUDA(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    h->chunk_events.push_back(ev);
+  }
+  // the copies may only overwrite the device rows once earlier work on the
+  // compute stream is done with them
+  MTP_CUDA(h, cudaEventRecord(h->chunk_events[nch], s));
+  MTP_CUDA(h, cudaStreamWaitEvent(h->copy_stream, h->chunk_events[nch], 0));
+  for (int k = 0; k < nch; ++k) {
+    const size_t lo = static_cast<size_t>(natoms) * k / nch, hi = static_cast<size_t>(natoms) * (k + 1) / nch;
+    const size_t n = hi - lo, r0 = lo * stride, nr = n * stride;
+    const cudaStream_t c = h->copy_stream;
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_itypes + lo, itypes + lo, n * sizeof(int), cudaMemcpyHostToDevice, c));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_rijs + 3 * r0, rijs + 3 * r0, 3 * nr * sizeof(double), cudaMemcpyHostToDevice, c));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_js + r0, js + r0, nr * sizeof(int), cudaMemcpyHostToDevice, c));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_jtypes + r0, jtypes + r0, nr * sizeof(int), cudaMemcpyHostToDevice, c));
+    if (counts) MTP_CUDA(h, cudaMemcpyAsync(h->d_counts + lo, counts + lo, n * sizeof(int), cudaMemcpyHostToDevice, c));
+    MTP_CUDA(h, cudaEventRecord(h->chunk_events[k], c));
+  }
+  cudaEvent_t e1 = nullptr;
+  for (int k = 0; k < nch; ++k) {
+    const int lo = static_cast<int>(static_cast<size_t>(natoms) * k / nch);
+    const int hi = static_cast<int>(static_cast<size_t>(natoms) * (k + 1) / nch);
+    MTP_CUDA(h, cudaStreamWaitEvent(s, h->chunk_events[k], 0));
+    if (k == 0) {
+      int st = prof_begin(h, &e1);
+      if (st != MTP_OK) return st;
+    }
+    int st = eval_range(h, lo, hi - lo, stride, h->d_itypes, h->d_rijs, h->d_jtypes, counts ? h->d_counts : nullptr);
+    if (st != MTP_OK) return st;
+  }
+  if (e1) MTP_CUDA(h, cudaEventRecord(e1, s));
+  MTP_CUDA(h, launch_incoming(natoms, stride, h->d_js, h->d_jtypes, counts ? h->d_counts : nullptr, h->d_in_cnt,
+                              h->d_in_ptr, h->d_in_cursor, h->d_in_slot, h->d_blk, s));
+  MTP_CUDA(h, launch_force_gather(natoms, stride, h->d_rijs, counts ? h->d_counts : nullptr, h->d_G, h->d_in_ptr,
+                                  h->d_in_slot, h->d_F, h->d_wown, vatom, s));
   return MTP_OK;
 }
 
@@ -626,15 +703,21 @@ int mtp_compute(mtp_handle* h, int natoms, int stride, const int* itypes, const 
   auto t0 = std::chrono::steady_clock::now();
   const size_t N = natoms, NS = N * stride;
   cudaStream_t s = h->stream;
-  if (natoms > 0) {
-    MTP_CUDA(h, cudaMemcpyAsync(h->d_itypes, itypes, N * sizeof(int), cudaMemcpyHostToDevice, s));
-    MTP_CUDA(h, cudaMemcpyAsync(h->d_rijs, rijs, 3 * NS * sizeof(double), cudaMemcpyHostToDevice, s));
-    MTP_CUDA(h, cudaMemcpyAsync(h->d_js, js, NS * sizeof(int), cudaMemcpyHostToDevice, s));
-    MTP_CUDA(h, cudaMemcpyAsync(h->d_jtypes, jtypes, NS * sizeof(int), cudaMemcpyHostToDevice, s));
-    if (counts) MTP_CUDA(h, cudaMemcpyAsync(h->d_counts, counts, N * sizeof(int), cudaMemcpyHostToDevice, s));
+  int st;
+  if (natoms >= kPipelineMinAtoms) {
+    st = run_host_pipelined(h, natoms, stride, itypes, rijs, js, jtypes, counts,
+                            (flags & MTP_VATOM) ? h->d_vatom : nullptr);
+  } else {
+    if (natoms > 0) {
+      MTP_CUDA(h, cudaMemcpyAsync(h->d_itypes, itypes, N * sizeof(int), cudaMemcpyHostToDevice, s));
+      MTP_CUDA(h, cudaMemcpyAsync(h->d_rijs, rijs, 3 * NS * sizeof(double), cudaMemcpyHostToDevice, s));
+      MTP_CUDA(h, cudaMemcpyAsync(h->d_js, js, NS * sizeof(int), cudaMemcpyHostToDevice, s));
+      MTP_CUDA(h, cudaMemcpyAsync(h->d_jtypes, jtypes, NS * sizeof(int), cudaMemcpyHostToDevice, s));
+      if (counts) MTP_CUDA(h, cudaMemcpyAsync(h->d_counts, counts, N * sizeof(int), cudaMemcpyHostToDevice, s));
+    }
+    st = run_device(h, natoms, stride, h->d_itypes, h->d_rijs, h->d_js, h->d_jtypes, counts ? h->d_counts : nullptr,
+                    true, h->d_F, (flags & MTP_VATOM) ? h->d_vatom : nullptr);
   }
-  int st = run_device(h, natoms, stride, h->d_itypes, h->d_rijs, h->d_js, h->d_jtypes, counts ? h->d_counts : nullptr,
-                      true, h->d_F, (flags & MTP_VATOM) ? h->d_vatom : nullptr);
   if (st != MTP_OK) return st;
   MTP_CUDA(h, launch_totals(natoms, h->d_E, h->d_wown, h->d_partials, h->d_tot, s));
   if (natoms > 0) {

@@ -198,6 +198,39 @@ def test_device_path_matches_host_path():
     assert np.array_equal(W.cpu().numpy(), host["virial"])
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_chunked_host_path_matches_device_path(precision):
+    """From 65,536 atoms on, mtp_compute copies host rows in chunks that
+    overlap the evaluation; the result must be bitwise the device path's
+    (the same kernel on every atom, the same fixed-order sums)."""
+    path = potential_path("cfg1md_L16_S2.mtp")
+    pot = read_mtp(path)
+    s = synth.config2_structure(26)          # 70,304 atoms
+    s.types = s.types % pot.species_count
+    N, stride = s.natoms, 64
+    d = torch.device("cuda")
+    with MTPEngine(path, N, stride, precision=precision) as eng:
+        x = torch.as_tensor(s.positions, device=d)
+        t = torch.as_tensor(s.types, dtype=torch.int32, device=d)
+        js = torch.empty((N, stride), dtype=torch.int32, device=d)
+        im, jt = torch.empty_like(js), torch.empty_like(js)
+        cnt = torch.empty(N, dtype=torch.int32, device=d)
+        rij = torch.empty((N, stride, 3), dtype=torch.float64, device=d)
+        eng.neighbors_device(x, s.cell, t, pot.max_dist + 0.3, stride, js, im, jt, cnt)
+        eng.pack_rij_device(x, s.cell, js, im, cnt, rij)
+        E, F, W = eng.compute_device(t, rij, js, jt, cnt)
+        torch.cuda.synchronize()
+        eng.sync_status()
+        host = eng.compute(t.cpu().numpy(), rij.cpu().numpy(), js.cpu().numpy(), jt.cpu().numpy(),
+                           cnt.cpu().numpy())
+        host2 = eng.compute(t.cpu().numpy(), rij.cpu().numpy(), js.cpu().numpy(), jt.cpu().numpy(),
+                            cnt.cpu().numpy())
+    assert float(E.cpu()[0]) == host["energy"] == host2["energy"]
+    assert np.array_equal(F.cpu().numpy(), host["forces"])
+    assert np.array_equal(W.cpu().numpy(), host["virial"])
+    assert np.array_equal(host["forces"], host2["forces"])
+
+
 def test_batched_configurations_match_oracle():
     path = potential_path("cfg3_L20_S2.mtp")
     pot = read_mtp(path)

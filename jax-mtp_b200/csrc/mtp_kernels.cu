@@ -3,6 +3,7 @@
 #include "mtp_launch.hpp"
 #include "mtp_md.hpp"
 
+#include <climits>
 #include <type_traits>
 
 namespace mtp {
@@ -208,19 +209,37 @@ __global__ void k_fill_incoming(int natoms, int stride, const int* js, const int
 }
 
 // Sort each atom's incoming list by slot id: the gather order, and so the
-// rounding of the forces, no longer depends on the fill race above.
+// rounding of the forces, no longer depends on the fill race above.  One warp
+// per atom: lists of up to 64 slots are ranked in registers (slot ids are
+// distinct, so each value's rank is the count of smaller values); longer
+// lists fall back to an insertion sort by the warp's first lane.
 __global__ void k_sort_incoming(int natoms, const int* in_ptr, int* in_slot) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= natoms) return;
-  const int b = in_ptr[k], e = in_ptr[k + 1];
-  for (int x = b + 1; x < e; ++x) {
-    const int v = in_slot[x];
-    int y = x - 1;
-    while (y >= b && in_slot[y] > v) {
-      in_slot[y + 1] = in_slot[y];
-      --y;
+  const int atom = static_cast<int>((blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (atom >= natoms) return;   // the whole warp leaves together
+  const int b = in_ptr[atom], n = in_ptr[atom + 1] - b;
+  if (n <= 64) {
+    const int v0 = lane < n ? in_slot[b + lane] : INT_MAX;
+    const int v1 = lane + 32 < n ? in_slot[b + lane + 32] : INT_MAX;
+    int r0 = 0, r1 = 0;
+    for (int k = 0; k < 32; ++k) {
+      const int u0 = __shfl_sync(0xffffffffu, v0, k), u1 = __shfl_sync(0xffffffffu, v1, k);
+      r0 += (u0 < v0) + (u1 < v0);
+      r1 += (u0 < v1) + (u1 < v1);
     }
-    in_slot[y + 1] = v;
+    __syncwarp();
+    if (lane < n) in_slot[b + r0] = v0;
+    if (lane + 32 < n) in_slot[b + r1] = v1;
+  } else if (lane == 0) {
+    for (int x = b + 1; x < b + n; ++x) {
+      const int v = in_slot[x];
+      int y = x - 1;
+      while (y >= b && in_slot[y] > v) {
+        in_slot[y + 1] = in_slot[y];
+        --y;
+      }
+      in_slot[y + 1] = v;
+    }
   }
 }
 
@@ -236,7 +255,8 @@ cudaError_t launch_incoming(int natoms, int stride, const int* js, const int* jt
   cudaError_t e = scan_exclusive(natoms, in_cnt, in_ptr, block_tmp, st);
   if (e != cudaSuccess) return e;
   k_fill_incoming<<<gb, 256, 0, st>>>(natoms, stride, js, jtypes, counts, in_ptr, in_cursor, in_slot);
-  k_sort_incoming<<<(natoms + 127) / 128, 128, 0, st>>>(natoms, in_ptr, in_slot);
+  k_sort_incoming<<<static_cast<unsigned>((static_cast<size_t>(natoms) * 32 + 255) / 256), 256, 0, st>>>(
+      natoms, in_ptr, in_slot);
   return cudaGetLastError();
 }
 

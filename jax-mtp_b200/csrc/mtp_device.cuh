@@ -117,7 +117,7 @@ __host__ __device__ inline SmemLayout smem_layout(int v_size, int M, int S, int 
   L.slot = take(sizeof(int) * n_pad * A);
   L.dmt = L.dmt_in_v ? L.v : take(sizeof(T) * R * Q * A);
   L.red = take(sizeof(double) * (threads / 32) * A);
-  L.cnt = take(sizeof(int) * (threads / 32 + 1));
+  L.cnt = take(sizeof(int) * (threads / 32 + 8));   // per-warp counts, then per-atom totals
   L.total = (o + 31) & ~size_t(31);
   return L;
 }
@@ -382,8 +382,8 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
     // moments that are read but never written (the force phase of the
     // previous atom may have reused their slots for its dense table)
     for (int x = tid; x < md.nzero * A; x += NT) V[(md.v_m + md.zero_list[x / A]) * A + x % A] = T(0);
-    int it_a[A], nv_a[A];
-    // ---- N1 + N2 per atom of the group -------------------------------------
+    int it_a[A], nv_a[A], cnt_a[A];
+    // ---- N1: staging of every atom of the block ---------------------------
 #pragma unroll
     for (int a = 0; a < A; ++a) {
       const int atom = base + a;
@@ -399,117 +399,146 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
         if (tid == 0) atomicOr(io.err, kErrCapacity);
         cnt = cnt < 0 ? 0 : n_pad;
       }
+      cnt_a[a] = cnt;
+      nv_a[a] = 0;
+    }
+    // tasks (atom, slot) with each atom's slots padded to whole warps, so a
+    // warp's ballot covers one atom; all atoms of the block in one sweep
+    const int S32 = (io.nbr_stride + 31) & ~31;
+    for (int v0 = 0; v0 < A * S32; v0 += NT) {
+      const int v = v0 + tid;
+      const int a = v < A * S32 ? v / S32 : A;
+      const int s = v - a * S32;
+      int it = 0, cnt = 0;
+#pragma unroll
+      for (int aa = 0; aa < A; ++aa)
+        if (aa == a) {
+          it = it_a[aa];
+          cnt = cnt_a[aa];
+        }
+      const int atom = base + a;
+      const bool real = a < A && atom < io.natoms;
       const size_t arow = static_cast<size_t>(real ? atom : 0) * io.nbr_stride;
       const double* rrow = io.rijs + arow * 3;
       const int* trow = io.jtypes + arow;
       double* grow = io.pair_grad + arow * 3;
-      T* sU = reinterpret_cast<T*>(smem + L.u) + static_cast<size_t>(a) * 4 * n_pad;
-      T* sF = reinterpret_cast<T*>(smem + L.f) + static_cast<size_t>(a) * R * n_pad;
-      T* sFp = reinterpret_cast<T*>(smem + L.fp) + static_cast<size_t>(a) * R * n_pad;
-      T* sPw = reinterpret_cast<T*>(smem + L.pw) + static_cast<size_t>(a) * pws * n_pad;
-      int* sSlot = reinterpret_cast<int*>(smem + L.slot) + a * n_pad;
-
-      int nv = 0;
-      for (int s0 = 0; s0 < io.nbr_stride; s0 += NT) {
-        const int s = s0 + tid;
-        bool valid = false;
-        T rx = T(0), ry = T(0), rz = T(0), d = T(0);
-        int jt = -1;
-        if (real && s < io.nbr_stride) {
-          if (s < cnt) {
-            jt = __ldg(trow + s);
-            rx = static_cast<T>(__ldg(rrow + 3 * s));
-            ry = static_cast<T>(__ldg(rrow + 3 * s + 1));
-            rz = static_cast<T>(__ldg(rrow + 3 * s + 2));
-            if (jt >= S) {
-              atomicOr(io.err, kErrSpecies);
-              jt = -1;
-            }
-            const T r2 = rx * rx + ry * ry + rz * rz;
-            d = dev_sqrt(r2);
-            valid = (jt >= 0) && (r2 > T(0)) && (d < rmax);
+      bool valid = false;
+      T rx = T(0), ry = T(0), rz = T(0), d = T(0);
+      int jt = -1;
+      if (real && s < io.nbr_stride) {
+        if (s < cnt) {
+          jt = __ldg(trow + s);
+          rx = static_cast<T>(__ldg(rrow + 3 * s));
+          ry = static_cast<T>(__ldg(rrow + 3 * s + 1));
+          rz = static_cast<T>(__ldg(rrow + 3 * s + 2));
+          if (jt >= S) {
+            atomicOr(io.err, kErrSpecies);
+            jt = -1;
           }
-          if (!valid) {
-            grow[3 * s] = 0.0;
-            grow[3 * s + 1] = 0.0;
-            grow[3 * s + 2] = 0.0;
-          }
+          const T r2 = rx * rx + ry * ry + rz * rz;
+          d = dev_sqrt(r2);
+          valid = (jt >= 0) && (r2 > T(0)) && (d < rmax);
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, valid);
-        const int w = tid >> 5, l = tid & 31;
-        if (l == 0) sCnt[w] = __popc(bal);
-        __syncthreads();
-        if (tid == 0) {
-          int accn = 0;
-          for (int i = 0; i < (NT >> 5); ++i) {
-            int c = sCnt[i];
-            sCnt[i] = accn;
-            accn += c;
-          }
-          sCnt[NT >> 5] = accn;
+        if (!valid) {
+          grow[3 * s] = 0.0;
+          grow[3 * s + 1] = 0.0;
+          grow[3 * s + 2] = 0.0;
         }
-        __syncthreads();
-        if (valid) {
-          const int q = nv + sCnt[w] + __popc(bal & ((1u << l) - 1u));
-          const T inv_d = T(1) / d;
-          const T ux = rx * inv_d, uy = ry * inv_d, uz = rz * inv_d;
-          sU[4 * q] = ux;
-          sU[4 * q + 1] = uy;
-          sU[4 * q + 2] = uz;
-          sU[4 * q + 3] = d;
-          sSlot[q] = s;
-          // Chebyshev T_n(x) and dT_n/dx by their recurrences, folded into
-          // sum_n c[t_i, t_j, mu, n] T_n for every mu as the terms appear
-          const T x = (T(2) * d - rsum) * inv_range;
-          const T dxdd = T(2) * inv_range;
-          const T* c = sRad + (static_cast<size_t>(it) * S + jt) * R * K;
-          T bas[kMaxR], dbas[kMaxR];
-#pragma unroll
-          for (int mu = 0; mu < kMaxR; ++mu) {
-            bas[mu] = mu < R ? c[mu * K] : T(0);   // T_0 = 1, T_0' = 0
-            dbas[mu] = T(0);
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, valid);
+      const int w = tid >> 5, l = tid & 31, nw = NT >> 5;
+      if (l == 0) sCnt[w] = __popc(bal);
+      __syncthreads();
+      if (tid == 0) {
+        // exclusive offsets of each warp within its atom's kept slots of this
+        // sweep; per-atom totals after the warp counts
+        int accn = 0, cur = -1;
+        for (int i = 0; i < nw; ++i) {
+          const int ai = (v0 + 32 * i) / S32;
+          if (ai != cur) {
+            if (cur >= 0 && cur < A) sCnt[nw + cur] = accn;
+            cur = ai;
+            accn = 0;
           }
-          T t_prev = T(1), t_cur = x, dt_prev = T(0), dt_cur = T(1);
-          for (int n = 1; n < K; ++n) {
+          const int c = sCnt[i];
+          sCnt[i] = accn;
+          accn += c;
+        }
+        if (cur >= 0 && cur < A) sCnt[nw + cur] = accn;
+      }
+      __syncthreads();
+      if (valid) {
+        int nv = 0;
 #pragma unroll
-            for (int mu = 0; mu < kMaxR; ++mu) {
-              if (mu < R) {
-                bas[mu] = dev_fma(c[mu * K + n], t_cur, bas[mu]);
-                dbas[mu] = dev_fma(c[mu * K + n], dt_cur, dbas[mu]);
-              }
-            }
-            const T t_next = T(2) * x * t_cur - t_prev;
-            const T dt_next = T(2) * t_cur + T(2) * x * dt_cur - dt_prev;
-            t_prev = t_cur;
-            t_cur = t_next;
-            dt_prev = dt_cur;
-            dt_cur = dt_next;
-          }
-          const T gap = rmax - d;
-          const T smooth = gap * gap;
+        for (int aa = 0; aa < A; ++aa)
+          if (aa == a) nv = nv_a[aa];
+        const int q = nv + sCnt[w] + __popc(bal & ((1u << l) - 1u));
+        T* sU = reinterpret_cast<T*>(smem + L.u) + static_cast<size_t>(a) * 4 * n_pad;
+        T* sF = reinterpret_cast<T*>(smem + L.f) + static_cast<size_t>(a) * R * n_pad;
+        T* sFp = reinterpret_cast<T*>(smem + L.fp) + static_cast<size_t>(a) * R * n_pad;
+        T* sPw = reinterpret_cast<T*>(smem + L.pw) + static_cast<size_t>(a) * pws * n_pad;
+        int* sSlot = reinterpret_cast<int*>(smem + L.slot) + a * n_pad;
+        const T inv_d = T(1) / d;
+        const T ux = rx * inv_d, uy = ry * inv_d, uz = rz * inv_d;
+        sU[4 * q] = ux;
+        sU[4 * q + 1] = uy;
+        sU[4 * q + 2] = uz;
+        sU[4 * q + 3] = d;
+        sSlot[q] = s;
+        // Chebyshev T_n(x) and dT_n/dx by their recurrences, folded into
+        // sum_n c[t_i, t_j, mu, n] T_n for every mu as the terms appear
+        const T x = (T(2) * d - rsum) * inv_range;
+        const T dxdd = T(2) * inv_range;
+        const T* c = sRad + (static_cast<size_t>(it) * S + jt) * R * K;
+        T bas[kMaxR], dbas[kMaxR];
+#pragma unroll
+        for (int mu = 0; mu < kMaxR; ++mu) {
+          bas[mu] = mu < R ? c[mu * K] : T(0);   // T_0 = 1, T_0' = 0
+          dbas[mu] = T(0);
+        }
+        T t_prev = T(1), t_cur = x, dt_prev = T(0), dt_cur = T(1);
+        for (int n = 1; n < K; ++n) {
 #pragma unroll
           for (int mu = 0; mu < kMaxR; ++mu) {
             if (mu < R) {
-              sF[q * R + mu] = scal * smooth * bas[mu];
-              sFp[q * R + mu] = scal * (T(-2) * gap * bas[mu] + smooth * dbas[mu] * dxdd);
+              bas[mu] = dev_fma(c[mu * K + n], t_cur, bas[mu]);
+              dbas[mu] = dev_fma(c[mu * K + n], dt_cur, dbas[mu]);
             }
           }
-          T* pw = sPw + q * pws;
-          T px = T(1), py = T(1), pz = T(1);
-          for (int e = 0; e < D1; ++e) {
-            pw[e] = px;
-            pw[D1 + e] = py;
-            pw[2 * D1 + e] = pz;
-            px *= ux;
-            py *= uy;
-            pz *= uz;
+          const T t_next = T(2) * x * t_cur - t_prev;
+          const T dt_next = T(2) * t_cur + T(2) * x * dt_cur - dt_prev;
+          t_prev = t_cur;
+          t_cur = t_next;
+          dt_prev = dt_cur;
+          dt_cur = dt_next;
+        }
+        const T gap = rmax - d;
+        const T smooth = gap * gap;
+#pragma unroll
+        for (int mu = 0; mu < kMaxR; ++mu) {
+          if (mu < R) {
+            sF[q * R + mu] = scal * smooth * bas[mu];
+            sFp[q * R + mu] = scal * (T(-2) * gap * bas[mu] + smooth * dbas[mu] * dxdd);
           }
         }
-        nv += sCnt[NT >> 5];
-        __syncthreads();
+        T* pw = sPw + q * pws;
+        T px = T(1), py = T(1), pz = T(1);
+        for (int e = 0; e < D1; ++e) {
+          pw[e] = px;
+          pw[D1 + e] = py;
+          pw[2 * D1 + e] = pz;
+          px *= ux;
+          py *= uy;
+          pz *= uz;
+        }
       }
-      nv_a[a] = nv;
-
+      // atoms touched by this sweep add its kept count
+#pragma unroll
+      for (int aa = 0; aa < A; ++aa) {
+        const int first = v0 / S32, last = (v0 + NT - 1) / S32;
+        if (aa >= first && aa <= last) nv_a[aa] += sCnt[nw + aa];
+      }
+      __syncthreads();
     }
     // ---- N2: basic moments m[(mu, a, b, c)] of every atom of the block ------
     // tasks (atom, monomial); monomials are sorted by degree, so the tasks of a

@@ -458,6 +458,19 @@ def run_train(args, device, dist):
                                           batch.volumes, batch.nconfig)
         loss = float(weighted_loss(E_p, F_p, S_p, (E_t, F_t, S_t)))
         eng3.sync_status()
+    # least-squares basis fit of configuration 3 (FP64): Jacobian by 289
+    # batched forwards, then a thin SVD (the reference's jacfwd + lstsq)
+    from mtp_b200.train import solve_lls_basis
+    with MTPEngine(os.path.join(potdir, "cfg3_L20_S2.mtp"), nd.natoms, nd.n_pad, precision="fp64") as e64:
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        theta, info = solve_lls_basis(e64, batch, (E_t, F_t, S_t), pot3.species_coeffs, pot3.radial_coeffs)
+        torch.cuda.synchronize(device)
+        lls_s = time.perf_counter() - t0
+        e64.sync_status()
+    out["cfg3_lls_basis"] = {"seconds": lls_s, "forwards": pot3.alpha_scalar_moments + 1, "rank": info["rank"],
+                             "loss_after": info["loss"], "loss_before": loss, "precision": "fp64",
+                             "rows": int(batch.nconfig * 7 + 3 * batch.natoms)}
     out["cfg3_batched_forward"] = {"value": world * batch.nconfig * steps / (ms * 1e-3), "unit": "cfg/s",
                                    "configs": batch.nconfig, "atoms": batch.natoms, "nbr_stride": nd.n_pad,
                                    "ms_per_batch": ms / steps, "precision": "mixed", "loss_vs_labels": loss,

@@ -823,9 +823,17 @@ int mtp_adjoint_batch_device(mtp_handle* h, int natoms, int stride, int nconfig,
   if (!d_gspecies || !d_gmoment || !d_gradial) return fail(h, MTP_E_INVALID, "null gradient pointer");
   if (natoms > 0 && (!d_itypes || !d_rijs || !d_js || !d_jtypes || !d_cfg || !d_volumes || !d_gE || !d_gF || !d_gS))
     return fail(h, MTP_E_INVALID, "null pointer");
+  // with the value space in global memory, 512 lanes give the SM twice the
+  // warps for the same L2 footprint
+  int lanes = h->threads;
   DeviceSchedule* ds = nullptr;
-  int st = get_schedule(h, h->threads, access_width(true, 1), &ds);
+  int st = get_schedule(h, lanes, access_width(true, 1), &ds);
   if (st != MTP_OK) return st;
+  if (lanes < 512 && !adjoint_fits_shared(make_model(h, *ds), stride, lanes)) {
+    lanes = 512;
+    st = get_schedule(h, lanes, access_width(true, 1), &ds);
+    if (st != MTP_OK) return st;
+  }
   DevModel md = make_model(h, *ds);
   TrainIO tio{};
   tio.natoms = natoms;
@@ -843,7 +851,7 @@ int mtp_adjoint_batch_device(mtp_handle* h, int natoms, int stride, int nconfig,
   tio.gS = d_gS;
   tio.err = h->d_err;
   std::string err;
-  cudaError_t ce = launch_adjoint(md, tio, h->threads, h->sm_count, h->train, d_gspecies, d_gmoment, d_gradial,
+  cudaError_t ce = launch_adjoint(md, tio, lanes, h->sm_count, h->train, d_gspecies, d_gmoment, d_gradial,
                                   h->stream, err);
   if (!err.empty()) return fail(h, MTP_E_CAPACITY, err);
   if (ce != cudaSuccess) return cuda_fail(h, ce, "adjoint");

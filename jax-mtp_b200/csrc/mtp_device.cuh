@@ -205,8 +205,35 @@ __device__ __forceinline__ void run_pass_n(const uint2* __restrict__ ent, int st
 }
 
 // Generic lane-program streamer (used by the dual-number kernels): every thread
-// walks its column of the [steps][lanes] entries with kPrefetch in flight
-// (steps is a multiple of kPrefetch, rows after a pass exist).
+// walks its column of the [steps][LANES] entries with kPrefetch in flight
+// (steps is a multiple of kPrefetch, rows after a pass exist; LANES fixed so
+// every request is one load at a constant offset).
+template <int LANES, typename Body>
+__device__ __forceinline__ void stream_entries_t(const uint2* __restrict__ ent, int steps, int tid, Body& body) {
+  const uint2* p = ent + tid;
+  uint2 buf[kPrefetch];
+#pragma unroll
+  for (int k = 0; k < kPrefetch; ++k) buf[k] = __ldg(p + k * LANES);
+  for (int s0 = 0; s0 < steps; s0 += kPrefetch) {
+    p += kPrefetch * LANES;
+#pragma unroll
+    for (int k = 0; k < kPrefetch; ++k) {
+      const uint2 e = buf[k];
+      buf[k] = __ldg(p + k * LANES);
+      body(e);
+    }
+  }
+}
+
+template <typename Body>
+__device__ __forceinline__ void stream_entries_n(const uint2* __restrict__ ent, int steps, int lanes, int tid,
+                                                 Body& body) {
+  if (lanes == 512) stream_entries_t<512>(ent, steps, tid, body);
+  else if (lanes == 256) stream_entries_t<256>(ent, steps, tid, body);
+  else stream_entries_t<128>(ent, steps, tid, body);
+}
+
+// Runtime-lane variant of stream_entries_t.
 template <typename Body>
 __device__ __forceinline__ void stream_entries(const uint2* __restrict__ ent, int steps, int lanes, int tid,
                                                Body& body) {

@@ -7,7 +7,7 @@ namespace mtp {
 
 struct TrainSmem {
   int pws;
-  size_t v, rad, u, du, f, fp, phi, phip, pw, A, Bv, jt, abc, mk, gth, gxi, grad, red, cnt, total;
+  size_t v, rad, u, du, f, fp, phi, phip, pw, A, Bv, jt, gxi, grad, red, cnt, total;
 };
 
 template <typename T>
@@ -34,9 +34,6 @@ __host__ __device__ inline TrainSmem train_layout(int v_size, int S, int R, int 
   L.A = take(sizeof(T) * R * n_pad);
   L.Bv = take(sizeof(T) * R * n_pad);
   L.jt = take(sizeof(int) * n_pad);
-  L.abc = take(sizeof(int) * 4 * P);
-  L.mk = take(sizeof(int) * kMaxR * P);
-  L.gth = take(sizeof(double) * Sa);
   L.gxi = take(sizeof(double) * S);
   L.grad = take(sizeof(double) * S * S * R * K);
   L.red = take(sizeof(double) * (threads / 32));
@@ -45,27 +42,38 @@ __host__ __device__ inline TrainSmem train_layout(int v_size, int S, int R, int 
   return L;
 }
 
+// A value and its tangent side by side, so one 16-byte access serves both.
+template <typename T>
+struct Dual2;
+template <>
+struct Dual2<double> {
+  using type = double2;
+  static __device__ __forceinline__ double2 make(double v, double t) { return make_double2(v, t); }
+};
+template <>
+struct Dual2<float> {
+  using type = float2;
+  static __device__ __forceinline__ float2 make(float v, float t) { return make_float2(v, t); }
+};
+
 // Forward pass on duals: (m3, dm3) += c * (m1 m2, dm1 m2 + m1 dm2).
 template <typename T>
 struct DualFwdBody {
-  T* V;
-  int H;
+  typename Dual2<T>::type* V;
   T acc, tac;
   __device__ __forceinline__ void operator()(const uint2 e) {
     const T c = entry_mult<T>(e.y);
-    const uint32_t a = e.x & 0xFFFFu, b = e.x >> 16;
-    const T va = V[a], vb = V[b], ta = V[a + H], tb = V[b + H];
-    acc = dev_fma(c * va, vb, acc);
-    tac = dev_fma(c, dev_fma(ta, vb, va * tb), tac);
+    const auto A = V[e.x & 0xFFFFu], B = V[e.x >> 16];
+    acc = dev_fma(c * A.x, B.x, acc);
+    tac = dev_fma(c, dev_fma(A.y, B.x, A.x * B.y), tac);
     const uint32_t op = (e.y >> kOpShift) & 3u;
     if (op) {
       const uint32_t d = e.y >> kDstShift;
       if (op == kOpStore) {
-        V[d] = acc;
-        V[d + H] = tac;
+        V[d] = Dual2<T>::make(acc, tac);
       } else {
-        V[d] += acc;
-        V[d + H] += tac;
+        const auto o = V[d];
+        V[d] = Dual2<T>::make(o.x + acc, o.y + tac);
       }
       acc = T(0);
       tac = T(0);
@@ -77,24 +85,21 @@ struct DualFwdBody {
 //   lambda_s += c (lambda_t m_o + tau_t dm_o),  tau_s += c tau_t m_o.
 template <typename T>
 struct DualRevBody {
-  T* V;
-  int H;
+  typename Dual2<T>::type* V;
   T acc, tac;
   __device__ __forceinline__ void operator()(const uint2 e) {
     const T c = entry_mult<T>(e.y);
-    const uint32_t a = e.x & 0xFFFFu, b = e.x >> 16;
-    const T la = V[a], ta = V[a + H], mb = V[b], tb = V[b + H];
-    acc = dev_fma(c, dev_fma(la, mb, ta * tb), acc);
-    tac = dev_fma(c * ta, mb, tac);
+    const auto A = V[e.x & 0xFFFFu], B = V[e.x >> 16];   // (lambda_t, tau_t), (m_o, dm_o)
+    acc = dev_fma(c, dev_fma(A.x, B.x, A.y * B.y), acc);
+    tac = dev_fma(c * A.y, B.x, tac);
     const uint32_t op = (e.y >> kOpShift) & 3u;
     if (op) {
       const uint32_t d = e.y >> kDstShift;
       if (op == kOpStore) {
-        V[d] = acc;
-        V[d + H] = tac;
+        V[d] = Dual2<T>::make(acc, tac);
       } else {
-        V[d] += acc;
-        V[d + H] += tac;
+        const auto o = V[d];
+        V[d] = Dual2<T>::make(o.x + acc, o.y + tac);
       }
       acc = T(0);
       tac = T(0);
@@ -107,10 +112,11 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
                                                      double* partials) {
   extern __shared__ __align__(32) unsigned char smem[];
   const int NT = blockDim.x, tid = threadIdx.x;
-  const int S = md.S, R = md.R, K = md.K, P = md.P, D1 = md.D + 1, H = md.v_size;
+  const int S = md.S, R = md.R, K = md.K, P = md.P, D1 = md.D + 1;
   const TrainSmem L = train_layout<T>(kVGlobal ? 0 : md.v_size, S, R, K, P, md.D, md.Sa, n_pad, NT);
-  T* V = kVGlobal ? reinterpret_cast<T*>(vscratch) + static_cast<size_t>(blockIdx.x) * 2 * md.v_size
-                  : reinterpret_cast<T*>(smem + L.v);
+  using T2 = typename Dual2<T>::type;
+  T2* V = kVGlobal ? reinterpret_cast<T2*>(vscratch) + static_cast<size_t>(blockIdx.x) * md.v_size
+                   : reinterpret_cast<T2*>(smem + L.v);
   T* sRad = reinterpret_cast<T*>(smem + L.rad);
   T* sU = reinterpret_cast<T*>(smem + L.u);
   T* sDu = reinterpret_cast<T*>(smem + L.du);
@@ -122,32 +128,27 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
   T* sA = reinterpret_cast<T*>(smem + L.A);
   T* sB = reinterpret_cast<T*>(smem + L.Bv);
   int* sJt = reinterpret_cast<int*>(smem + L.jt);
-  int* sAbc = reinterpret_cast<int*>(smem + L.abc);
-  int* sMk = reinterpret_cast<int*>(smem + L.mk);
-  double* gTh = reinterpret_cast<double*>(smem + L.gth);
   double* gXi = reinterpret_cast<double*>(smem + L.gxi);
   double* gRad = reinterpret_cast<double*>(smem + L.grad);
   int* sCnt = reinterpret_cast<int*>(smem + L.cnt);
   const int pws = L.pws;
   const int nrad = S * S * R * K;
+  // this block's partial gradients [Sa | S | S*S*R*K]; the moment part is
+  // accumulated here directly (each thread owns the same coefficients for
+  // every atom), species and radial parts in shared memory
+  double* out = partials + static_cast<size_t>(blockIdx.x) * (md.Sa + S + nrad);
+  const int4* mono_abc = reinterpret_cast<const int4*>(md.mono_abc);
 
   for (int x = tid; x < nrad; x += NT) {
     sRad[x] = static_cast<T>(md.radial[x]);
     gRad[x] = 0.0;
   }
-  for (int x = tid; x < 4 * P; x += NT) sAbc[x] = md.mono_abc[x];
-  for (int x = tid; x < kMaxR * P; x += NT) sMk[x] = md.mono_k[x];
-  for (int x = tid; x < md.Sa; x += NT) gTh[x] = 0.0;
+  for (int x = tid; x < md.Sa; x += NT) out[x] = 0.0;
   for (int x = tid; x < S; x += NT) gXi[x] = 0.0;
-  for (int x = tid; x < md.nzero; x += NT) {
-    V[md.v_m + md.zero_list[x]] = T(0);
-    V[md.v_m + md.zero_list[x] + H] = T(0);
-  }
+  for (int x = tid; x < md.nzero; x += NT) V[md.v_m + md.zero_list[x]] = Dual2<T>::make(T(0), T(0));
   if (tid == 0) {
-    V[md.v_zero] = T(0);
-    V[md.v_one] = T(1);
-    V[md.v_zero + H] = T(0);
-    V[md.v_one + H] = T(0);
+    V[md.v_zero] = Dual2<T>::make(T(0), T(0));
+    V[md.v_one] = Dual2<T>::make(T(1), T(0));
   }
   const T rmax = static_cast<T>(md.rmax);
   const T inv_range = static_cast<T>(1.0 / (md.rmax - md.rmin));
@@ -300,7 +301,8 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
 
     // ---- N2: basic moments and their tangents ------------------------------
     for (int p = tid; p < P; p += NT) {
-      const int a = sAbc[4 * p], b = sAbc[4 * p + 1], cc = sAbc[4 * p + 2];
+      const int4 abc = __ldg(mono_abc + p);
+      const int a = abc.x, b = abc.y, cc = abc.z;
       const T am = static_cast<T>(a), bm = static_cast<T>(b), cm = static_cast<T>(cc);
       T acc[kMaxR], tac[kMaxR];
 #pragma unroll
@@ -329,41 +331,34 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
 #pragma unroll
       for (int mu = 0; mu < kMaxR; ++mu) {
         if (mu < R) {
-          const int k = sMk[kMaxR * p + mu];
-          if (k >= 0) {
-            V[md.v_m + k] = acc[mu];
-            V[md.v_m + k + H] = tac[mu];
-          }
+          const int k = __ldg(md.mono_k + kMaxR * p + mu);
+          if (k >= 0) V[md.v_m + k] = Dual2<T>::make(acc[mu], tac[mu]);
         }
       }
     }
-    for (int x = tid; x < md.M; x += NT) {
-      V[md.v_dm + x] = T(0);
-      V[md.v_dm + x + H] = T(0);
-    }
+    for (int x = tid; x < md.M; x += NT) V[md.v_dm + x] = Dual2<T>::make(T(0), T(0));
     __syncthreads();
     for (int x = tid; x < md.nseed; x += NT) {
       const T sv = static_cast<T>(md.seed_val[x]);
-      V[md.v_dm + md.seed_idx[x]] = a_i * sv;
-      V[md.v_dm + md.seed_idx[x] + H] = sv;
+      V[md.v_dm + md.seed_idx[x]] = Dual2<T>::make(a_i * sv, sv);
     }
 
     // ---- dual forward tree --------------------------------------------------
     for (int ps = 0; ps < md.nfwd; ++ps) {
-      DualFwdBody<T> body{V, H, T(0), T(0)};
-      stream_entries(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, body);
+      DualFwdBody<T> body{V, T(0), T(0)};
+      stream_entries_n(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, body);
       __syncthreads();
     }
     for (int a = tid; a < md.Sa; a += NT) {
-      const int k = md.v_m + __ldg(md.mapping + a);
-      gTh[a] += static_cast<double>(a_i) * static_cast<double>(V[k]) + static_cast<double>(V[k + H]);
+      const T2 v = V[md.v_m + __ldg(md.mapping + a)];
+      out[a] += static_cast<double>(a_i) * static_cast<double>(v.x) + static_cast<double>(v.y);
     }
     if (tid == 0) gXi[it] += static_cast<double>(a_i);
 
     // ---- dual reverse tree ---------------------------------------------------
     for (int ps = 0; ps < md.nrev; ++ps) {
-      DualRevBody<T> body{V, H, T(0), T(0)};
-      stream_entries(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, body);
+      DualRevBody<T> body{V, T(0), T(0)};
+      stream_entries_n(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, body);
       __syncthreads();
     }
 
@@ -387,7 +382,8 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
           const T* pw = sPw + q * pws;
           const T* du = sDu + 4 * q;
           for (int p = sl; p < P; p += tpn) {
-            const int a = sAbc[4 * p], b = sAbc[4 * p + 1], cc = sAbc[4 * p + 2];
+            const int4 abc = __ldg(mono_abc + p);
+            const int a = abc.x, b = abc.y, cc = abc.z;
             const T px = pw[a], py = pw[D1 + b], pz = pw[2 * D1 + cc];
             const T mono = px * py * pz;
             const T dmono = static_cast<T>(a) * pw[a > 0 ? a - 1 : 0] * py * pz * du[0] +
@@ -396,11 +392,11 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
 #pragma unroll
             for (int mu = 0; mu < kMaxR; ++mu) {
               if (mu < R) {
-                const int k = sMk[kMaxR * p + mu];
+                const int k = __ldg(md.mono_k + kMaxR * p + mu);
                 if (k >= 0) {
-                  const T lam = V[md.v_dm + k], tau = V[md.v_dm + k + H];
-                  GA[mu] = dev_fma(lam, mono, dev_fma(tau, dmono, GA[mu]));
-                  GB[mu] = dev_fma(tau, mono, GB[mu]);
+                  const T2 lt = V[md.v_dm + k];   // (lambda, tau)
+                  GA[mu] = dev_fma(lt.x, mono, dev_fma(lt.y, dmono, GA[mu]));
+                  GB[mu] = dev_fma(lt.y, mono, GB[mu]);
                 }
               }
             }
@@ -437,10 +433,7 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
     }
     __syncthreads();
   }
-  // per-block partials: [Sa | S | S*S*R*K]
-  const int np = md.Sa + S + nrad;
-  double* out = partials + static_cast<size_t>(blockIdx.x) * np;
-  for (int x = tid; x < md.Sa; x += NT) out[x] = gTh[x];
+  // per-block partials: [Sa | S | S*S*R*K] (the moment part is already there)
   for (int x = tid; x < S; x += NT) out[md.Sa + x] = gXi[x];
   for (int x = tid; x < nrad; x += NT) out[md.Sa + S + x] = gRad[x];
 }
@@ -489,6 +482,11 @@ static int adjoint_occupancy(size_t bytes, int threads) {
   return nb;
 }
 
+bool adjoint_fits_shared(const DevModel& md, int n_pad, int threads) {
+  const TrainSmem L = train_layout<double>(md.v_size, md.S, md.R, md.K, md.P, md.D, md.Sa, n_pad, threads);
+  return adjoint_occupancy<false>(L.total, threads) > 0;
+}
+
 cudaError_t launch_adjoint(const DevModel& md, const TrainIO& io, int threads, int sm_count, TrainWorkspace& ws,
                            double* gspecies, double* gmoment, double* gradial, cudaStream_t st, std::string& err) {
   const int n_pad = io.nbr_stride;
@@ -506,7 +504,17 @@ cudaError_t launch_adjoint(const DevModel& md, const TrainIO& io, int threads, i
     err = "the adjoint block does not fit in shared memory for this basis and nbr_stride";
     return cudaSuccess;
   }
-  const int blocks = std::max(1, std::min(io.natoms, bps * sm_count));
+  int blocks = std::max(1, std::min(io.natoms, bps * sm_count));
+  if (vglobal) {
+    // the blocks' global value spaces should stay resident in L2: cap their
+    // total at 5/8 of it (but keep one block per SM)
+    int dev = 0, l2 = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
+    const size_t per = static_cast<size_t>(2) * md.v_size * sizeof(double);
+    const int cap = static_cast<int>(std::max<size_t>(sm_count, (static_cast<size_t>(l2) * 5 / 8) / per));
+    blocks = std::max(1, std::min(blocks, cap));
+  }
   const size_t need_p = static_cast<size_t>(blocks) * np;
   if (need_p > ws.partials_cap) {
     if (ws.partials) cudaFree(ws.partials);

@@ -49,6 +49,10 @@ struct TrainWorkspace {
 
 void train_free(TrainWorkspace& w);
 
+// Whether the adjoint's value space (value and tangent of every slot) fits in
+// shared memory for `threads` lanes; otherwise it lives in global memory.
+bool adjoint_fits_shared(const DevModel& md, int n_pad, int threads);
+
 // Runs the adjoint kernel (FP64) and the fixed-order reduction into the outputs.
 cudaError_t launch_adjoint(const DevModel& md, const TrainIO& io, int threads, int sm_count, TrainWorkspace& ws,
                            double* gspecies, double* gmoment, double* gradial, cudaStream_t st, std::string& err);

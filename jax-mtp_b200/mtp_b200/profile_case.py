@@ -33,8 +33,13 @@ def main(argv=None):
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--apb", type=int, default=0, help="atoms per block (0: automatic)")
     ap.add_argument("--sweep", action="store_true", help="time every (threads, atoms per block) shape")
+    ap.add_argument("--training", type=int, default=0,
+                    help="instead: a batch of this many training configurations (synth.training_batch, "
+                         "32-512 atoms, seed 8); one batched forward, then --calls adjoint launches")
     a = ap.parse_args(argv)
     pot = read_mtp(a.potential)
+    if a.training:
+        return training_case(a, pot)
     s = synth.config2_structure(a.reps)
     s.types = s.types % pot.species_count
     dev = torch.device("cuda")
@@ -66,6 +71,28 @@ def main(argv=None):
             eng.sync_status()
             print(json.dumps({"atoms": N, "precision": a.precision, "eval_ms_per_call": ms / max(1, n),
                               "launch": eng.launch()}), flush=True)
+
+
+def training_case(a, pot):
+    """Batched forward + adjoint (training gradient) on synthetic configurations."""
+    from .train import DeviceBatch
+    dev = torch.device("cuda")
+    structs = synth.training_batch(a.training, 32, 512, pot.species_count, seed=8)
+    nds = [synth.build_neighbors(st, pot.max_dist) for st in structs]
+    nd, cfg, _, vols = synth.pack_batch(nds)
+    b = DeviceBatch.from_numpy(nd, cfg, vols, device=dev)
+    with MTPEngine(a.potential, nd.natoms, nd.n_pad, precision=a.precision) as eng:
+        E, F, S = eng.batch_device(b.itypes, b.rijs, b.js, b.jtypes, b.counts, b.cfg, b.volumes, b.nconfig)
+        gE, gF, gS = torch.ones_like(E), 0.01 * torch.ones_like(F), 0.001 * torch.ones_like(S)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.calls):
+            eng.adjoint_device(b.itypes, b.rijs, b.js, b.jtypes, b.counts, b.cfg, b.volumes, b.nconfig, gE, gF, gS)
+        e1.record()
+        torch.cuda.synchronize()
+        eng.sync_status()
+        print(json.dumps({"configs": b.nconfig, "atoms": nd.natoms, "n_pad": nd.n_pad,
+                          "adjoint_ms_per_call": e0.elapsed_time(e1) / max(1, a.calls)}), flush=True)
 
 
 if __name__ == "__main__":

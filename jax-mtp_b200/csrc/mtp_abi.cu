@@ -276,14 +276,17 @@ int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, 
       }
     }
     if (best < 0) {
+      // value space in global memory: 512 lanes give an SM 16 warps with one
+      // block, so the blocks' value spaces stay within L2
+      const int lanes = 512;
       DeviceSchedule* ds = nullptr;
-      int st = get_schedule(h, h->threads, access_width(fp64, 1), &ds);
+      int st = get_schedule(h, lanes, access_width(fp64, 1), &ds);
       if (st != MTP_OK) return st;
-      int bps = eval_blocks_per_sm(make_model(h, *ds), stride, h->threads, fp64, true, 1);
+      int bps = eval_blocks_per_sm(make_model(h, *ds), stride, lanes, fp64, true, 1);
       if (h->blocks_per_sm > 0) bps = std::min(bps, h->blocks_per_sm);
       if (bps <= 0)
         return fail(h, MTP_E_CAPACITY, "the evaluation block does not fit in shared memory for this basis and max_nbr");
-      c = mtp_handle::LaunchChoice{h->threads, bps, true, 0, 1};
+      c = mtp_handle::LaunchChoice{lanes, std::min(bps, 1), true, 0, 1};
     }
     DeviceSchedule* ds = nullptr;
     int st = get_schedule(h, c.lanes, access_width(fp64, c.A), &ds);

@@ -130,7 +130,10 @@ int mtp_execute_potential(mtp_handle* h, int natoms, int nneigh_total,
  * jtype < 0).  nbr_stride <= max_nbr.  Outputs selected by flags; pointers of
  * unselected outputs may be NULL.  forces [natoms][3] is always written.
  * virial [6] (LAMMPS order), eatom [natoms], vatom [natoms][6].
- * Synchronous: returns when results are in host memory.
+ * Synchronous: returns when results are in host memory.  From 65,536 atoms on,
+ * the inputs are copied in atom chunks on a second, library-owned stream while
+ * the evaluation runs on the chunks already copied (pinned host buffers let
+ * the copies overlap; results are bitwise those of mtp_compute_device).
  */
 int mtp_compute(mtp_handle* h, int natoms, int nbr_stride, const int* itypes, const double* rijs,
                 const int* js, const int* jtypes, const int* counts, int flags, double* energy,

@@ -91,7 +91,8 @@ def test_deterministic_bitwise():
     assert np.array_equal(a["virial"], b["virial"])
 
 
-SHAPES = [(128, 1), (256, 1), (512, 1), (256, 2), (512, 2), (256, 4), (512, 4)]
+# (128, 4): 4 atoms x 64 staged slots exceed 128 lanes, so staging takes two sweeps
+SHAPES = [(128, 1), (256, 1), (512, 1), (128, 2), (256, 2), (512, 2), (128, 4), (256, 4), (512, 4)]
 
 
 @pytest.mark.parametrize("threads,apb", SHAPES)

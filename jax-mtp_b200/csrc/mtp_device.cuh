@@ -155,8 +155,11 @@ __device__ __forceinline__ double entry_mult<double>(uint32_t y) {
 // multiple of kPrefetch and the program holds kPrefetch rows after any pass,
 // so nothing is bounds-tested.  Each entry feeds A atoms:
 // acc[a] += c * V[x][a] * V[y][a]; STORE/ADD flush into V[d][a].
+// Operands are read through Vr and flushes go through V: a pass never reads a
+// slot that it writes, so the two views do not alias.
 template <typename T, int A, int LANES>
-__device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int steps, int tid, T* __restrict__ V) {
+__device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int steps, int tid, T* __restrict__ V,
+                                         const T* __restrict__ Vr) {
   static_assert(kPrefetch == kStepAlign, "prefetch depth must equal the pass step alignment");
   const uint2* p = ent + tid;
   uint2 buf[kPrefetch];
@@ -172,8 +175,8 @@ __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int step
       const uint2 e = buf[k];
       buf[k] = __ldg(p + k * LANES);
       const T c = entry_mult<T>(e.y);
-      const Pack<T, A> va = *reinterpret_cast<const Pack<T, A>*>(V + (e.x & 0xFFFFu) * A);
-      const Pack<T, A> vb = *reinterpret_cast<const Pack<T, A>*>(V + (e.x >> 16) * A);
+      const Pack<T, A> va = *reinterpret_cast<const Pack<T, A>*>(Vr + (e.x & 0xFFFFu) * A);
+      const Pack<T, A> vb = *reinterpret_cast<const Pack<T, A>*>(Vr + (e.x >> 16) * A);
 #pragma unroll
       for (int a = 0; a < A; ++a) acc[a] = dev_fma(c * va.v[a], vb.v[a], acc[a]);
       if (e.y & (3u << kOpShift)) {
@@ -199,9 +202,9 @@ __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int step
 template <typename T, int A>
 __device__ __forceinline__ void run_pass_n(const uint2* __restrict__ ent, int steps, int lanes, int tid,
                                            T* __restrict__ V) {
-  if (lanes == 512) run_pass<T, A, 512>(ent, steps, tid, V);
-  else if (lanes == 256) run_pass<T, A, 256>(ent, steps, tid, V);
-  else run_pass<T, A, 128>(ent, steps, tid, V);
+  if (lanes == 512) run_pass<T, A, 512>(ent, steps, tid, V, V);
+  else if (lanes == 256) run_pass<T, A, 256>(ent, steps, tid, V, V);
+  else run_pass<T, A, 128>(ent, steps, tid, V, V);
 }
 
 // Generic lane-program streamer (used by the dual-number kernels): every thread

@@ -57,13 +57,17 @@ struct Dual2<float> {
 };
 
 // Forward pass on duals: (m3, dm3) += c * (m1 m2, dm1 m2 + m1 dm2).
+// Operands are read through Vr and flushes go through V: a pass never reads
+// a slot that it writes, so the two views do not alias (which lets the loads
+// of later entries move ahead of earlier flushes).
 template <typename T>
 struct DualFwdBody {
-  typename Dual2<T>::type* V;
+  typename Dual2<T>::type* __restrict__ V;
+  const typename Dual2<T>::type* __restrict__ Vr;
   T acc, tac;
   __device__ __forceinline__ void operator()(const uint2 e) {
     const T c = entry_mult<T>(e.y);
-    const auto A = V[e.x & 0xFFFFu], B = V[e.x >> 16];
+    const auto A = Vr[e.x & 0xFFFFu], B = Vr[e.x >> 16];
     acc = dev_fma(c * A.x, B.x, acc);
     tac = dev_fma(c, dev_fma(A.y, B.x, A.x * B.y), tac);
     const uint32_t op = (e.y >> kOpShift) & 3u;
@@ -85,11 +89,12 @@ struct DualFwdBody {
 //   lambda_s += c (lambda_t m_o + tau_t dm_o),  tau_s += c tau_t m_o.
 template <typename T>
 struct DualRevBody {
-  typename Dual2<T>::type* V;
+  typename Dual2<T>::type* __restrict__ V;
+  const typename Dual2<T>::type* __restrict__ Vr;
   T acc, tac;
   __device__ __forceinline__ void operator()(const uint2 e) {
     const T c = entry_mult<T>(e.y);
-    const auto A = V[e.x & 0xFFFFu], B = V[e.x >> 16];   // (lambda_t, tau_t), (m_o, dm_o)
+    const auto A = Vr[e.x & 0xFFFFu], B = Vr[e.x >> 16];   // (lambda_t, tau_t), (m_o, dm_o)
     acc = dev_fma(c, dev_fma(A.x, B.x, A.y * B.y), acc);
     tac = dev_fma(c * A.y, B.x, tac);
     const uint32_t op = (e.y >> kOpShift) & 3u;
@@ -345,7 +350,7 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
 
     // ---- dual forward tree --------------------------------------------------
     for (int ps = 0; ps < md.nfwd; ++ps) {
-      DualFwdBody<T> body{V, T(0), T(0)};
+      DualFwdBody<T> body{V, V, T(0), T(0)};
       stream_entries_n(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, body);
       __syncthreads();
     }
@@ -357,7 +362,7 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
 
     // ---- dual reverse tree ---------------------------------------------------
     for (int ps = 0; ps < md.nrev; ++ps) {
-      DualRevBody<T> body{V, T(0), T(0)};
+      DualRevBody<T> body{V, V, T(0), T(0)};
       stream_entries_n(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, body);
       __syncthreads();
     }

@@ -236,25 +236,6 @@ __device__ __forceinline__ void stream_entries_n(const uint2* __restrict__ ent, 
   else stream_entries_t<128>(ent, steps, tid, body);
 }
 
-// Runtime-lane variant of stream_entries_t.
-template <typename Body>
-__device__ __forceinline__ void stream_entries(const uint2* __restrict__ ent, int steps, int lanes, int tid,
-                                               Body& body) {
-  const uint2* p = ent + tid;
-  uint2 buf[kPrefetch];
-#pragma unroll
-  for (int k = 0; k < kPrefetch; ++k) buf[k] = __ldg(p + static_cast<size_t>(k) * lanes);
-  for (int s0 = 0; s0 < steps; s0 += kPrefetch) {
-    p += static_cast<size_t>(kPrefetch) * lanes;
-#pragma unroll
-    for (int k = 0; k < kPrefetch; ++k) {
-      const uint2 e = buf[k];
-      buf[k] = __ldg(p + static_cast<size_t>(k) * lanes);
-      body(e);
-    }
-  }
-}
-
 // Force-phase sums of two neighbours over this thread's share of the
 // monomial simplex.  With W_s = sum_mu Dm[s][mu] f_mu(d), W'_s the same with
 // f'_mu, and Q(u) = sum_s W_s u_x^a u_y^b u_z^c over slots s = (a, b, c):

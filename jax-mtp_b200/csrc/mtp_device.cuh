@@ -1,23 +1,28 @@
 // mtp_device.cuh - sm_100a kernels of the MTP evaluator.
 //
-// One persistent thread block evaluates one centre atom at a time (a
-// grid-stride loop over atoms):
+// One persistent thread block evaluates A centre atoms at a time (a
+// grid-stride loop over groups of A atoms):
 //
-//   N1  neighbour staging: slots of the atom's padded row are read with
-//       coalesced loads, tested (t_j >= 0, |r| < max_dist), compacted with a
-//       warp ballot, and each kept neighbour gets its unit vector, distance,
-//       radial functions f_mu(d), f'_mu(d) (Chebyshev basis times the smooth
-//       cutoff, jax_backend.py:83-95, 108-160) and the powers of its unit
-//       vector components, all in shared memory;
+//   N1  neighbour staging: the slots of the atoms' padded rows are read with
+//       coalesced loads in one sweep, tested (t_j >= 0, |r| < max_dist),
+//       compacted with warp ballots, and each kept neighbour gets its unit
+//       vector, distance, radial functions f_mu(d), f'_mu(d) (Chebyshev basis
+//       times the smooth cutoff, jax_backend.py:83-95, 108-160) and the powers
+//       of its unit vector components, all in shared memory;
 //   N2  basic moments m[(mu, a, b, c)] = sum_j f_mu(d_j) u_x^a u_y^b u_z^c
-//       (conversion.py:66-81), one thread per distinct monomial;
+//       (conversion.py:66-81), one thread per (atom, monomial), only the
+//       radial functions that have a moment at the monomial's degree;
 //   T   contraction tree (conversion.py:95-102) by the lane programs of the
 //       schedule, then E_i = xi[t_i] + theta . m[mapping] (jax_backend.py:101-106);
 //   R   reverse programs: dE_i/dm for every moment, gathered per source, so
 //       no two threads ever add into the same value;
-//   N3  per neighbour: dE_i/dr_ij from dE_i/dm of the basic moments
-//       (the analytic form of jax.value_and_grad at jax_backend.py:56),
+//   N3  per neighbour: dE_i/dr_ij from dE_i/dm of the basic moments by nested
+//       Horner over the monomial simplex (the analytic form of
+//       jax.value_and_grad at jax_backend.py:56), two neighbours per thread,
 //       written to the per-slot gradient array.
+//
+// The A atoms of a block share every lane-program entry: their values are
+// interleaved [slot][atom] so one vector access serves all of them.
 //
 // Forces then come from a per-atom gather (k_force_gather): the atom's own
 // slot gradients minus the gradients of the slots that point at it, in a

@@ -60,7 +60,7 @@ struct mtp_handle {
   // potential tables on the device
   double *d_radial = nullptr, *d_species = nullptr, *d_theta = nullptr, *d_seed_val = nullptr;
   int *d_mapping = nullptr, *d_seed_idx = nullptr, *d_zero = nullptr, *d_abc = nullptr, *d_mk = nullptr;
-  int *d_pair_base = nullptr, *d_dense_k = nullptr;
+  int* d_dense_k = nullptr;
   int nseed = 0;
   // input / output / scratch buffers sized by the capacities
   int *d_itypes = nullptr, *d_js = nullptr, *d_jtypes = nullptr, *d_counts = nullptr;
@@ -132,7 +132,6 @@ DevModel make_model(mtp_handle* h, const DeviceSchedule& ds) {
   md.nzero = static_cast<int>(s.zero_list.size());
   md.mono_abc = h->d_abc;
   md.mono_k = h->d_mk;
-  md.pair_base = h->d_pair_base;
   md.dense_k = h->d_dense_k;
   md.Q = s.Q;
   md.npairs = s.npairs;
@@ -179,9 +178,6 @@ int get_schedule(mtp_handle* h, int lanes, int width, DeviceSchedule** out) {
       MTP_CUDA(h, dalloc(&h->d_mk, ds.sched.mono_k.size()));
       MTP_CUDA(h, cudaMemcpy(h->d_mk, ds.sched.mono_k.data(), ds.sched.mono_k.size() * sizeof(int),
                              cudaMemcpyHostToDevice));
-      MTP_CUDA(h, dalloc(&h->d_pair_base, ds.sched.pair_base.size()));
-      MTP_CUDA(h, cudaMemcpy(h->d_pair_base, ds.sched.pair_base.data(), ds.sched.pair_base.size() * sizeof(int),
-                             cudaMemcpyHostToDevice));
       MTP_CUDA(h, dalloc(&h->d_dense_k, ds.sched.dense_k.size()));
       MTP_CUDA(h, cudaMemcpy(h->d_dense_k, ds.sched.dense_k.data(), ds.sched.dense_k.size() * sizeof(int),
                              cudaMemcpyHostToDevice));
@@ -215,7 +211,7 @@ void free_handle(mtp_handle* h) {
   auto F = [](void* p) { if (p) cudaFree(p); };
   for (auto& kv : h->scheds) F(kv.second.d_entries);
   F(h->d_radial); F(h->d_species); F(h->d_theta); F(h->d_seed_val);
-  F(h->d_mapping); F(h->d_seed_idx); F(h->d_zero); F(h->d_abc); F(h->d_mk); F(h->d_pair_base); F(h->d_dense_k);
+  F(h->d_mapping); F(h->d_seed_idx); F(h->d_zero); F(h->d_abc); F(h->d_mk); F(h->d_dense_k);
   F(h->d_itypes); F(h->d_js); F(h->d_jtypes); F(h->d_counts); F(h->d_rijs);
   F(h->d_G); F(h->d_E); F(h->d_F); F(h->d_wown); F(h->d_vatom);
   F(h->d_in_cnt); F(h->d_in_ptr); F(h->d_in_cursor); F(h->d_in_slot); F(h->d_blk);
@@ -386,7 +382,7 @@ int run_device(mtp_handle* h, int natoms, int stride, const int* itypes, const d
 
 // Systems from this size on are copied in chunks that overlap the evaluation.
 constexpr int kPipelineMinAtoms = 65536;
-constexpr int kPipelineChunks = 8;
+constexpr int kPipelineChunks = 16;
 
 // run_device for host input buffers: the inputs of chunk k go up on the copy
 // stream while the evaluation kernel works on chunk k-1 (events order each

@@ -59,7 +59,6 @@ struct DevModel {
   const int* zero_list;     // [nzero]
   const int* mono_abc;      // [P][4]
   const int* mono_k;        // [P][kMaxR]
-  const int* pair_base;     // [npairs] first dense slot of each (a, b) pair
   const int* dense_k;       // [Q][kMaxR] basic moment of dense slot and mu, or -1
   int nseed, nzero;
   int S, R, K, M, B, P, D, Sa;
@@ -252,7 +251,7 @@ __device__ __forceinline__ void stream_entries_n(const uint2* __restrict__ ent, 
 // pairs in snake order (sl, 2 tpn-1-sl, 2 tpn+sl, ...) of the pair order
 // (a + b ascending), so their shares differ by one pair at most.
 template <typename T, int R>
-__device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, const int* __restrict__ pair_base, int D,
+__device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
                                         int npairs, int D1, const T* __restrict__ fq0, const T* __restrict__ fpq0,
                                         const T* __restrict__ fq1, const T* __restrict__ fpq1, bool two,
                                         const T* __restrict__ pw0, const T* __restrict__ pw1, T uz0, T uz1, int sl,
@@ -265,16 +264,20 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, const int* __
     f1[mu] = two ? fq1[mu] : T(0);
     fp1[mu] = two ? fpq1[mu] : T(0);
   }
-  int s = 0, sb = 0;   // diagonal a + b of the current pair and its first pair index
+  // diagonal s = a + b of the current pair, its first pair index, and the
+  // first dense slot of the diagonal (pair order: each pair of diagonal s
+  // owns D - s + 1 slots, so slot bases follow without a table lookup)
+  int s = 0, sb = 0, slot_sb = 0;
   for (int k = 0;; ++k) {
     const int i = (k >> 1) * 2 * tpn + ((k & 1) ? 2 * tpn - 1 - sl : sl);
     if (i >= npairs) break;
     while (i >= sb + s + 1) {
       sb += s + 1;
+      slot_sb += (s + 1) * (D - s + 1);
       ++s;
     }
     const int ea = i - sb, eb = s - ea, top = D - s;
-    const T* drow = dmt + (__ldg(pair_base + i) + top) * R;
+    const T* drow = dmt + (slot_sb + ea * (D - s + 1) + top) * R;
     T h0 = T(0), hz0 = T(0), hs0 = T(0), h1 = T(0), hz1 = T(0), hs1 = T(0);
 #pragma unroll 2
     for (int c = top; c >= 0; --c, drow -= R) {
@@ -676,7 +679,7 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
           switch (R) {
 #define MTP_N3_CASE(RR)                                                                                        \
   case RR:                                                                                                     \
-    n3_sums<T, RR>(dmt, md.pair_base, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R, sFp + qb * R, \
+    n3_sums<T, RR>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R, sFp + qb * R, \
                    two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2], sU[4 * qb + 2], sl, tpn, Ssum, Gx, Gy, Gz); \
     break;
             MTP_N3_CASE(1) MTP_N3_CASE(2) MTP_N3_CASE(3) MTP_N3_CASE(4)

@@ -498,14 +498,12 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
   // dense simplex in pair order
   s.npairs = (s.D + 1) * (s.D + 2) / 2;
   s.Q = (s.D + 1) * (s.D + 2) * (s.D + 3) / 6;
-  s.pair_base.assign(s.npairs, 0);
   s.dense_k.assign(static_cast<size_t>(s.Q) * kMaxR, -1);
   {
-    int slot = 0, i = 0;
+    int slot = 0;
     for (int sum = 0; sum <= s.D; ++sum) {
-      for (int a = 0; a <= sum; ++a, ++i) {
+      for (int a = 0; a <= sum; ++a) {
         const int b = sum - a;
-        s.pair_base[i] = slot;
         for (int c = 0; c <= s.D - sum; ++c, ++slot) {
           auto it = mono_of.find(std::make_tuple(a, b, c));
           if (it == mono_of.end()) continue;

@@ -87,7 +87,6 @@ struct Schedule {
   // slots c = 0 .. D - s.  Used by the force phase (nested Horner in z, y).
   int Q = 0;                    // (D+1)(D+2)(D+3)/6 slots
   int npairs = 0;               // (D+1)(D+2)/2 pairs
-  std::vector<int> pair_base;   // [npairs] first slot of each pair's run
   std::vector<int> dense_k;     // [Q][kMaxR] basic-moment index of slot and mu, or -1
   std::vector<int> zero_list;   // non-basic moments never written (must read as 0)
   std::vector<Pass> fwd, rev;   // passes in execution order

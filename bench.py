@@ -353,6 +353,18 @@ def run_ours(args):
     achieved = flops / k_mixed / 1e12
     achieved64 = flops / k_64 / 1e12
     traffic = read_traffic()
+    # the same launch against HBM: algorithmic bytes per atom-step through the
+    # evaluation (28 n_pad + 36: r_ij and neighbour index in, force and energy out)
+    alg_bytes = (28 * STRIDE + 36) * N
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            hbm_peak = float(json.load(fh)["hbm_gbs"])
+        hbm_src = "MEASURED_PEAKS.json"
+    except (OSError, ValueError, KeyError):
+        hbm_peak, hbm_src = 6650.0, "fallback"
+    hbm_view = {"achieved_gbs": alg_bytes / k_mixed / 1e9, "peak_gbs": hbm_peak,
+                "frac": alg_bytes / k_mixed / 1e9 / hbm_peak, "algorithmic_bytes_per_launch": alg_bytes,
+                "peak_source": hbm_src}
     nrebuild = sum(1 for k in range(args.warmup + 1, args.warmup + args.steps + 1) if k % REBUILD == 0)
     launches = nrebuild * launches_per_step(True) + (args.steps - nrebuild) * launches_per_step(False)
 
@@ -388,7 +400,7 @@ def run_ours(args):
             "roofline": {"bound": "fp32-fma", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
                          "kernel": "k_mtp_eval<float> (mixed)", "flops_per_launch": flops,
-                         "kernel_ms": k_mixed * 1e3,
+                         "kernel_ms": k_mixed * 1e3, "hbm_view": hbm_view,
                          "peak_source": "measured live: FP32 FMA-chain kernel (no FP32/FP64 CUDA-core peak in "
                                         "MEASURED_PEAKS.json)",
                          "fp64_kernel": {"achieved": achieved64, "peak": fp64_peak, "frac": achieved64 / fp64_peak

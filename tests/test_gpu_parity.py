@@ -225,11 +225,15 @@ def test_chunked_host_path_matches_device_path(precision):
         host = eng.compute(t.cpu().numpy(), rij.cpu().numpy(), js.cpu().numpy(), jt.cpu().numpy(),
                            cnt.cpu().numpy())
         host2 = eng.compute(t.cpu().numpy(), rij.cpu().numpy(), js.cpu().numpy(), jt.cpu().numpy(),
-                            cnt.cpu().numpy())
+                            cnt.cpu().numpy(), eatom=True, vatom=True)
     assert float(E.cpu()[0]) == host["energy"] == host2["energy"]
     assert np.array_equal(F.cpu().numpy(), host["forces"])
     assert np.array_equal(W.cpu().numpy(), host["virial"])
     assert np.array_equal(host["forces"], host2["forces"])
+    # per-atom energies and virials of the chunked path sum to the totals
+    assert abs(host2["site_energies"].sum() - host2["energy"]) <= 1e-9 * abs(host2["energy"])
+    np.testing.assert_allclose(host2["vatom"].sum(0), host2["virial"], rtol=1e-9,
+                               atol=1e-9 * np.abs(host2["virial"]).max())
 
 
 def test_batched_configurations_match_oracle():

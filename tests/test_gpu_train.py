@@ -197,7 +197,22 @@ def test_cfg_to_lls_to_lbfgs_pipeline(tmp_path):
         with torch.no_grad():
             L1 = float(weighted_loss(*predict(params, eng, batch), tt))
         out = fit_lbfgs(eng, batch, tt, params, steps=30)
+        with torch.no_grad():
+            E_fit, F_fit, _ = predict(params, eng, batch)
         eng.sync_status()
+    # write-out: the trained potential reloaded in a new engine predicts the same
+    from mtp_b200.mtp_file import write_mtp
+    trained = pot.copy()
+    trained.species_coeffs = params["species"].detach().cpu().numpy()
+    trained.moment_coeffs = params["basis"].detach().cpu().numpy()
+    trained.radial_coeffs = params["radial"].detach().cpu().numpy()
+    write_mtp(tmp_path / "trained.mtp", trained)
+    with MTPEngine(str(tmp_path / "trained.mtp"), batch.natoms, int(batch.rijs.shape[1])) as eng2:
+        E2, F2, _ = eng2.batch_device(batch.itypes, batch.rijs, batch.js, batch.jtypes, batch.counts, batch.cfg,
+                                      batch.volumes, batch.nconfig)
+        eng2.sync_status()
+    assert _rel(E2.cpu().numpy(), E_fit.cpu().numpy()) <= 1e-12
+    assert _rel(F2.cpu().numpy(), F_fit.cpu().numpy()) <= 1e-10
     assert L1 < L0
     assert abs(L1 - info["loss"]) <= 1e-6 * L1
     hist = out["loss_history"]

@@ -389,8 +389,8 @@ constexpr int kPipelineChunks = 16;
 // chunk's kernel after its copies); the incoming lists and the force gather
 // need every row and follow the last chunk.  With pinned host buffers the
 // copies overlap the kernels; pageable ones are still correct.
-int run_host_pipelined(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
-                       const int* jtypes, const int* counts, double* vatom) {
+int run_host_pipelined_body(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs,
+                            const int* js, const int* jtypes, const int* counts, double* vatom) {
   const cudaStream_t s = h->stream;
   if (!h->copy_stream) MTP_CUDA(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
   const int nch = std::max(1, std::min(kPipelineChunks, natoms / (kPipelineMinAtoms / 2)));
@@ -432,6 +432,15 @@ int run_host_pipelined(mtp_handle* h, int natoms, int stride, const int* itypes,
   MTP_CUDA(h, launch_force_gather(natoms, stride, h->d_rijs, counts ? h->d_counts : nullptr, h->d_G, h->d_in_ptr,
                                   h->d_in_slot, h->d_F, h->d_wown, vatom, s));
   return MTP_OK;
+}
+
+// A failure part-way leaves copies from the caller's host buffers in flight:
+// they finish before the call returns, so the caller may free the buffers.
+int run_host_pipelined(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
+                       const int* jtypes, const int* counts, double* vatom) {
+  const int st = run_host_pipelined_body(h, natoms, stride, itypes, rijs, js, jtypes, counts, vatom);
+  if (st != MTP_OK && h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+  return st;
 }
 
 int read_err_flags(mtp_handle* h) {

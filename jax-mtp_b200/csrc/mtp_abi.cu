@@ -726,7 +726,10 @@ int mtp_compute(mtp_handle* h, int natoms, int stride, const int* itypes, const 
     st = run_device(h, natoms, stride, h->d_itypes, h->d_rijs, h->d_js, h->d_jtypes, counts ? h->d_counts : nullptr,
                     true, h->d_F, (flags & MTP_VATOM) ? h->d_vatom : nullptr);
   }
-  if (st != MTP_OK) return st;
+  if (st != MTP_OK) {
+    cudaStreamSynchronize(s);   // copies from the caller's buffers complete before the error returns
+    return st;
+  }
   MTP_CUDA(h, launch_totals(natoms, h->d_E, h->d_wown, h->d_partials, h->d_tot, s));
   if (natoms > 0) {
     MTP_CUDA(h, cudaMemcpyAsync(forces, h->d_F, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));

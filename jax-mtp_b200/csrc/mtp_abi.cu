@@ -103,8 +103,17 @@ int fail(mtp_handle* h, int code, const std::string& msg) {
   return code;
 }
 
+// A CUDA call failed: record it, and let work already queued on the handle's
+// streams (copies from or to the caller's host buffers among it) finish
+// before the error returns, so the caller may reuse or free those buffers.
 int cuda_fail(mtp_handle* h, cudaError_t e, const char* what) {
-  return fail(h, MTP_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  const int st = fail(h, MTP_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  if (h) {
+    cudaStreamSynchronize(h->stream);
+    if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+    cudaGetLastError();
+  }
+  return st;
 }
 
 #define MTP_CUDA(h, call)                                  \

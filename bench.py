@@ -373,6 +373,10 @@ def run_ours(args):
     if rank == 0 and not args.skip_e2e:
         e2e = run_e2e(eng["mixed"], mds["mixed"], N, args)
 
+    pair_call = None
+    if rank == 0 and not args.skip_e2e:
+        pair_call = run_pair_call(args)
+
     cpu = None
     if rank == 0 and not args.skip_cpu:
         cpu = cpu_baseline(pot, s, seconds=args.cpu_seconds)
@@ -407,6 +411,7 @@ def run_ours(args):
                                          if fp64_peak else None, "kernel_ms": k_64 * 1e3}},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "pair_style_call": pair_call,
             "gpu_launches": launches * 1,
             "clocks": clocks,
         }
@@ -566,6 +571,76 @@ def run_e2e(eng, md, N, args):
     return {"value": N * steps / dt, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "steps": steps, "api": "mtp_compute (C ABI, pinned host buffers, synchronous)",
             "note": "force call per MD step as the pair style makes it; integration not included"}
+
+
+def run_pair_call(args):
+    """Latency of one force call of the LAMMPS MD case: level-16 MTP, 2 species
+    (cfg1_L16_S2.mtp), bcc a = 2.87 A, 10^3 cells = 2,000 atoms, 50/50 species,
+    MAX_ATOMS_PER_NEIGHBOR 60, cutoff 5.0 A.  Host buffers in and out, as the pair
+    style calls it: through mtp_compute with page-locked rows (mtp_host_alloc,
+    what pair_mtp_b200.cpp packs into) and with pageable numpy arrays, and
+    through mtp_execute_potential (the reference bridge's per-atom row pointers,
+    built once outside the timed calls).  Host wall clock per synchronous call."""
+    import ctypes
+    from mtp_b200 import synth
+    from mtp_b200._lib import EFLAG, VFLAG, check, lib
+    from mtp_b200.engine import MTPEngine, pinned_empty
+    path = os.path.join(ROOT, "tests", "golden", "potentials", "cfg1_L16_S2.mtp")
+    s = synth.config1()
+    nd = synth.build_neighbors(s, 5.0, n_pad=60)
+    N, n = nd.js.shape
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    it = np.ascontiguousarray(nd.itypes, np.int32)
+    rij = np.ascontiguousarray(nd.rijs, np.float64)
+    js = np.ascontiguousarray(nd.js, np.int32)
+    jt = np.ascontiguousarray(nd.jtypes, np.int32)
+    cnt = np.ascontiguousarray(nd.counts, np.int32)
+    F = np.zeros((N, 3))
+    e = np.zeros(1)
+    vir = np.zeros(6)
+    st = np.zeros(6)
+    pinned = {}
+    for k, a in (("it", it), ("rij", rij), ("js", js), ("jt", jt), ("cnt", cnt), ("F", F), ("e", e), ("vir", vir)):
+        pinned[k] = pinned_empty(a.shape, a.dtype)
+        pinned[k][...] = a
+    Pv = ctypes.c_void_p * N
+    pr = Pv(*[rij[i].ctypes.data for i in range(N)])
+    pj = Pv(*[js[i].ctypes.data for i in range(N)])
+    pt = Pv(*[jt[i].ctypes.data for i in range(N)])
+    pf = Pv(*[F[i].ctypes.data for i in range(N)])
+    calls = max(20, min(200, 10 * args.steps))
+    out = {"workload": "level-16 MTP, 2 species, bcc a=2.87 A 10^3 = 2,000 atoms, 60 slots per row, cutoff 5.0 A",
+           "calls": calls, "timer": "host wall clock per synchronous call (H2D + kernels + D2H)"}
+    for prec in ("fp64", "mixed"):
+        with MTPEngine(path, N, n, precision=prec) as eng:
+            h = eng.handle
+
+            def flat():
+                check(lib().mtp_compute(h, N, n, P(it), P(rij), P(js), P(jt), P(cnt), EFLAG | VFLAG, P(e), P(F),
+                                        P(vir), None, None), h)
+
+            def flat_pinned():
+                b = pinned
+                check(lib().mtp_compute(h, N, n, P(b["it"]), P(b["rij"]), P(b["js"]), P(b["jt"]), P(b["cnt"]),
+                                        EFLAG | VFLAG, P(b["e"]), P(b["F"]), P(b["vir"]), None, None), h)
+
+            def bridge():
+                check(lib().mtp_execute_potential(h, N, int(cnt.sum()), ctypes.cast(pr, ctypes.c_void_p), P(it),
+                                                  ctypes.cast(pj, ctypes.c_void_p), P(cnt),
+                                                  ctypes.cast(pt, ctypes.c_void_p), float(nd.volume), P(e),
+                                                  ctypes.cast(pf, ctypes.c_void_p), P(st)), h)
+
+            for name, fn in (("mtp_compute_pinned", flat_pinned), ("mtp_compute_pageable", flat),
+                             ("mtp_execute_potential", bridge)):
+                for _ in range(5):
+                    fn()
+                t0 = time.perf_counter()
+                for _ in range(calls):
+                    fn()
+                us = (time.perf_counter() - t0) / calls * 1e6
+                out[f"{prec}_{name}_us"] = us
+                out[f"{prec}_{name}_atom_steps_per_s"] = N / (us * 1e-6)
+    return out
 
 
 def main():

@@ -273,6 +273,19 @@ int mtp_compute_device_noalloc(mtp_handle* h, int natoms, int nbr_stride, const 
  * (TFLOP/s, an FMA counted as 2 flops).  Used for the roofline. */
 int mtp_measure_fma_peak(double* fp64_tflops, double* fp32_tflops);
 
+/*
+ * Page-locked host memory for the host-buffer entry points.  A caller that
+ * packs its rows (rijs, js, jtypes, counts, itypes) and receives its outputs
+ * in these buffers lets mtp_compute move them by DMA instead of through the
+ * driver's staging copy of pageable memory.  The reference's pool refilled
+ * pageable NumPy arrays every step (zero_overhead.cpp:61-117); this replaces
+ * that pool's storage.  bytes == 0 gives *out == NULL.  Errors: MTP_E_INVALID,
+ * MTP_E_OOM, MTP_E_CUDA (text in mtp_last_error(NULL)).  mtp_host_free(NULL)
+ * is a no-op.
+ */
+int mtp_host_alloc(size_t bytes, void** out);
+int mtp_host_free(void* p);
+
 #ifdef __cplusplus
 }
 #endif

@@ -984,6 +984,30 @@ int mtp_measure_fma_peak(double* fp64, double* fp32) {
   return measure_fma_peak(fp64, fp32) == cudaSuccess ? MTP_OK : MTP_E_CUDA;
 }
 
+int mtp_host_alloc(size_t bytes, void** out) {
+  if (!out) return fail(nullptr, MTP_E_INVALID, "mtp_host_alloc: null output pointer");
+  *out = nullptr;
+  if (bytes == 0) return MTP_OK;
+  const cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    return fail(nullptr, e == cudaErrorMemoryAllocation ? MTP_E_OOM : MTP_E_CUDA,
+                std::string("mtp_host_alloc: ") + cudaGetErrorString(e));
+  }
+  return MTP_OK;
+}
+
+int mtp_host_free(void* p) {
+  if (!p) return MTP_OK;
+  const cudaError_t e = cudaFreeHost(p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(nullptr, MTP_E_CUDA, std::string("mtp_host_free: ") + cudaGetErrorString(e));
+  }
+  return MTP_OK;
+}
+
 }  // extern "C"
 
 // ===========================================================================

@@ -18,7 +18,8 @@
 //       no two threads ever add into the same value;
 //   N3  per neighbour: dE_i/dr_ij from dE_i/dm of the basic moments by nested
 //       Horner over the monomial simplex (the analytic form of
-//       jax.value_and_grad at jax_backend.py:56), two neighbours per thread,
+//       jax.value_and_grad at jax_backend.py:56), two neighbours per thread
+//       in FP32 and one in FP64,
 //       written to the per-slot gradient array.
 //
 // The A atoms of a block share every lane-program entry: their values are
@@ -240,17 +241,17 @@ __device__ __forceinline__ void stream_entries_n(const uint2* __restrict__ ent, 
   else stream_entries_t<128>(ent, steps, tid, body);
 }
 
-// Force-phase sums of two neighbours over this thread's share of the
-// monomial simplex.  With W_s = sum_mu Dm[s][mu] f_mu(d), W'_s the same with
+// Force-phase sums of one or (kTwo) two neighbours over this thread's share
+// of the monomial simplex.  With W_s = sum_mu Dm[s][mu] f_mu(d), W'_s the same with
 // f'_mu, and Q(u) = sum_s W_s u_x^a u_y^b u_z^c over slots s = (a, b, c):
 //   G = grad_u Q = (Gx, Gy, Gz),   S = sum_s W'_s u_x^a u_y^b u_z^c.
 // Each (a, b) pair is a Horner chain in u_z over c = D-a-b .. 0 (value and
 // z-derivative), scaled by the stored powers of u_x and u_y.  The dE/dm rows
-// are per atom, so the two neighbours share every row load and their chains
-// run side by side.  The tpn threads of a neighbour pair take the (a, b)
+// are per atom, so two neighbours share every row load and their chains run
+// side by side.  The tpn threads of a neighbour pair take the (a, b)
 // pairs in snake order (sl, 2 tpn-1-sl, 2 tpn+sl, ...) of the pair order
 // (a + b ascending), so their shares differ by one pair at most.
-template <typename T, int R>
+template <typename T, int R, bool kTwo>
 __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
                                         int npairs, int D1, const T* __restrict__ fq0, const T* __restrict__ fpq0,
                                         const T* __restrict__ fq1, const T* __restrict__ fpq1, bool two,
@@ -261,8 +262,8 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
   for (int mu = 0; mu < R; ++mu) {
     f0[mu] = fq0[mu];
     fp0[mu] = fpq0[mu];
-    f1[mu] = two ? fq1[mu] : T(0);
-    fp1[mu] = two ? fpq1[mu] : T(0);
+    f1[mu] = kTwo && two ? fq1[mu] : T(0);
+    fp1[mu] = kTwo && two ? fpq1[mu] : T(0);
   }
   // diagonal s = a + b of the current pair, its first pair index, and the
   // first dense slot of the diagonal (pair order: each pair of diagonal s
@@ -279,7 +280,7 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
     const int ea = i - sb, eb = s - ea, top = D - s;
     const T* drow = dmt + (slot_sb + ea * (D - s + 1) + top) * R;
     T h0 = T(0), hz0 = T(0), hs0 = T(0), h1 = T(0), hz1 = T(0), hs1 = T(0);
-#pragma unroll 2
+#pragma unroll 1
     for (int c = top; c >= 0; --c, drow -= R) {
       T w0 = T(0), wp0 = T(0), w1 = T(0), wp1 = T(0);
 #pragma unroll
@@ -287,15 +288,19 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
         const T g = drow[mu];
         w0 = dev_fma(g, f0[mu], w0);
         wp0 = dev_fma(g, fp0[mu], wp0);
-        w1 = dev_fma(g, f1[mu], w1);
-        wp1 = dev_fma(g, fp1[mu], wp1);
+        if (kTwo) {
+          w1 = dev_fma(g, f1[mu], w1);
+          wp1 = dev_fma(g, fp1[mu], wp1);
+        }
       }
       hz0 = dev_fma(hz0, uz0, h0);
       h0 = dev_fma(h0, uz0, w0);
       hs0 = dev_fma(hs0, uz0, wp0);
-      hz1 = dev_fma(hz1, uz1, h1);
-      h1 = dev_fma(h1, uz1, w1);
-      hs1 = dev_fma(hs1, uz1, wp1);
+      if (kTwo) {
+        hz1 = dev_fma(hz1, uz1, h1);
+        h1 = dev_fma(h1, uz1, w1);
+        hs1 = dev_fma(hs1, uz1, wp1);
+      }
     }
     {
       const T xa = pw0[ea], yb = pw0[D1 + eb];
@@ -307,7 +312,7 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
       Gz[0] = dev_fma(xy, hz0, Gz[0]);
       S[0] = dev_fma(xy, hs0, S[0]);
     }
-    {
+    if (kTwo) {
       const T xa = pw1[ea], yb = pw1[D1 + eb];
       const T dxa = ea > 0 ? static_cast<T>(ea) * pw1[ea - 1] : T(0);
       const T dyb = eb > 0 ? static_cast<T>(eb) * pw1[D1 + eb - 1] : T(0);
@@ -660,8 +665,11 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
       const T* sPw = reinterpret_cast<T*>(smem + L.pw) + static_cast<size_t>(a) * pws * n_pad;
       const int* sSlot = reinterpret_cast<int*>(smem + L.slot) + a * n_pad;
       double* grow = io.pair_grad + static_cast<size_t>(atom < io.natoms ? atom : 0) * io.nbr_stride * 3;
-      // threads take pairs of neighbours (q, q + nt)
-      const int nt = (nv + 1) >> 1;
+      // FP32: threads take pairs of neighbours (q, q + nt), which share every
+      // table-row load; FP64: one neighbour per thread (the second
+      // neighbour's registers would spill at the 128-register budget)
+      constexpr bool kTwoN = sizeof(T) == 4;
+      const int nt = kTwoN ? (nv + 1) >> 1 : nv;
       int tpn = 32;
       while (tpn > 1 && tpn * nt > NT) tpn >>= 1;
       const int total = nt * tpn;
@@ -670,7 +678,7 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
         const bool active = idx < total;
         const int q0 = active ? idx / tpn : 0;
         const int q1 = q0 + nt;
-        const bool two = active && q1 < nv;
+        const bool two = kTwoN && active && q1 < nv;
         const int sl = idx & (tpn - 1);
         T Ssum[2] = {T(0), T(0)}, Gx[2] = {T(0), T(0)}, Gy[2] = {T(0), T(0)}, Gz[2] = {T(0), T(0)};
         if (active) {
@@ -679,7 +687,7 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
           switch (R) {
 #define MTP_N3_CASE(RR)                                                                                        \
   case RR:                                                                                                     \
-    n3_sums<T, RR>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R, sFp + qb * R, \
+    n3_sums<T, RR, kTwoN>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R, sFp + qb * R, \
                    two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2], sU[4 * qb + 2], sl, tpn, Ssum, Gx, Gy, Gz); \
     break;
             MTP_N3_CASE(1) MTP_N3_CASE(2) MTP_N3_CASE(3) MTP_N3_CASE(4)

@@ -51,6 +51,8 @@ SIGNATURES = {
     "mtp_profile": (_I, [_P, _I]),
     "mtp_profile_read": (_I, [_P, ctypes.POINTER(_D), ctypes.POINTER(_I)]),
     "mtp_compute_device_noalloc": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "mtp_host_alloc": (_I, [ctypes.c_size_t, ctypes.POINTER(_P)]),
+    "mtp_host_free": (_I, [_P]),
 }
 
 _lib = None

@@ -17,7 +17,7 @@ import numpy as np
 from . import _lib
 from ._lib import EATOM, EFLAG, REUSE_NEIGHBORS, VATOM, VFLAG, check, lib
 
-__all__ = ["MTPEngine", "stress_from_virial", "virial_from_stress"]
+__all__ = ["MTPEngine", "pinned_empty", "stress_from_virial", "virial_from_stress"]
 
 
 def _ptr(a: Optional[np.ndarray]):
@@ -26,6 +26,30 @@ def _ptr(a: Optional[np.ndarray]):
 
 def _c(a, dtype) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=dtype)
+
+
+class _PinnedBlock:
+    """Page-locked bytes from mtp_host_alloc, freed with the last array viewing them."""
+
+    def __init__(self, nbytes: int):
+        p = ctypes.c_void_p()
+        check(lib().mtp_host_alloc(nbytes, ctypes.byref(p)), None)
+        self.ptr = p.value
+        self.__array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (self.ptr, False), "version": 3}
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            lib().mtp_host_free(self.ptr)
+            self.ptr = None
+
+
+def pinned_empty(shape, dtype=np.float64) -> np.ndarray:
+    """Uninitialised page-locked host array: ``compute`` moves it by DMA
+    instead of through the driver's staging copy of pageable memory."""
+    dt = np.dtype(dtype)
+    n = int(np.prod(shape, dtype=np.int64)) * dt.itemsize
+    raw = np.asarray(_PinnedBlock(max(n, dt.itemsize)))
+    return raw[:n].view(dt).reshape(shape)
 
 
 def stress_from_virial(virial: np.ndarray, volume: float) -> np.ndarray:

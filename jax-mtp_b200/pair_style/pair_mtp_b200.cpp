@@ -66,14 +66,10 @@ void PairMTPB200::grow_buffers()
   const size_t rows = static_cast<size_t>(max_atoms);
   const size_t slots = rows * max_nbr;
   if (rij.size() != 3 * slots) {
-    rij.assign(3 * slots, 0.0);
-    js.assign(slots, -1);
-    jtypes.assign(slots, -1);
-    counts.assign(rows, 0);
-    itypes.assign(rows, 0);
-    fbuf.assign(3 * rows, 0.0);
-    ebuf.assign(rows, 0.0);
-    vbuf.assign(6 * rows, 0.0);
+    const bool ok = rij.assign(3 * slots, 0.0) && js.assign(slots, -1) && jtypes.assign(slots, -1) &&
+        counts.assign(rows, 0) && itypes.assign(rows, 0) && fbuf.assign(3 * rows, 0.0) &&
+        ebuf.assign(rows, 0.0) && vbuf.assign(6 * rows, 0.0);
+    if (!ok) error->one(FLERR, std::string("pair jax/mtp: page-locked buffers: ") + mtp_last_error(nullptr));
   }
 }
 

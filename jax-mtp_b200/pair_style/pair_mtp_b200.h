@@ -21,13 +21,46 @@ PairStyle(jax/mtp,PairMTPB200);
 #ifndef LMP_PAIR_MTP_B200_H
 #define LMP_PAIR_MTP_B200_H
 
+#include <cstddef>
 #include <vector>
 
+#include "mtp_b200.h"
 #include "pair.h"
 
-struct mtp_handle;
-
 namespace LAMMPS_NS {
+
+// Page-locked host array from mtp_host_alloc: the rows the pair style packs
+// here reach the GPU by DMA, without the driver's staging copy of pageable
+// memory.  Reallocates only when the size changes.
+template <typename T> class PinnedArray {
+ public:
+  PinnedArray() = default;
+  ~PinnedArray() { mtp_host_free(p_); }
+  PinnedArray(const PinnedArray &) = delete;
+  PinnedArray &operator=(const PinnedArray &) = delete;
+  // n elements, each set to v; false if the allocation failed
+  bool assign(size_t n, T v)
+  {
+    if (n != n_) {
+      mtp_host_free(p_);
+      p_ = nullptr;
+      n_ = 0;
+      void *q = nullptr;
+      if (mtp_host_alloc(n * sizeof(T), &q) != MTP_OK) return false;
+      p_ = static_cast<T *>(q);
+      n_ = n;
+    }
+    for (size_t i = 0; i < n_; ++i) p_[i] = v;
+    return true;
+  }
+  size_t size() const { return n_; }
+  T *data() { return p_; }
+  T &operator[](size_t i) { return p_[i]; }
+
+ private:
+  T *p_ = nullptr;
+  size_t n_ = 0;
+};
 
 class PairMTPB200 : public Pair {
  public:
@@ -53,10 +86,11 @@ class PairMTPB200 : public Pair {
   mtp_handle *handle;
   long long total_calls;
 
-  // persistent flat buffers [max_atoms][max_nbr] (no per-step allocation)
-  std::vector<double> rij;
-  std::vector<int> js, jtypes, counts, itypes;
-  std::vector<double> fbuf, ebuf, vbuf;
+  // persistent flat buffers [max_atoms][max_nbr] in page-locked memory (no
+  // per-step allocation)
+  PinnedArray<double> rij;
+  PinnedArray<int> js, jtypes, counts, itypes;
+  PinnedArray<double> fbuf, ebuf, vbuf;
   std::vector<int> tag_to_local;
 };
 

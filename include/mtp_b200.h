@@ -104,6 +104,14 @@ int mtp_use_own_stream(mtp_handle* h);
  * alpha_index_times_count, alpha_scalar_moments, max monomial degree. */
 int mtp_get_info(const mtp_handle* h, int* out8);
 
+/* Call statistics: out4 = {host-buffer calls (mtp_compute and the bridge),
+ * their total host time in ms, CUDA graphs captured for mtp_compute, graph
+ * replays}.  Below 65,536 atoms, mtp_compute with page-locked host buffers
+ * (mtp_host_alloc, cudaHostRegister) captures its copies and kernels as one
+ * CUDA graph on the second consecutive call with the same arguments and
+ * replays it while they repeat. */
+int mtp_get_stats(const mtp_handle* h, double* out4);
+
 /* Replace the coefficients (training updates): species [S], moment [Sa], radial [S*S*R*K]
  * in .mtp order.  Any pointer may be NULL to keep the current values. */
 int mtp_set_coeffs(mtp_handle* h, const double* species_coeffs, const double* moment_coeffs,
@@ -133,7 +141,11 @@ int mtp_execute_potential(mtp_handle* h, int natoms, int nneigh_total,
  * Synchronous: returns when results are in host memory.  From 65,536 atoms on,
  * the inputs are copied in atom chunks on a second, library-owned stream while
  * the evaluation runs on the chunks already copied (pinned host buffers let
- * the copies overlap; results are bitwise those of mtp_compute_device).
+ * the copies overlap; results are bitwise those of mtp_compute_device).  Below
+ * that, with every host buffer page-locked and the handle on a non-default
+ * stream, the second consecutive call with the same arguments is captured as
+ * one CUDA graph (copies, kernels, read-backs) and replayed while the
+ * arguments repeat; the buffers' contents may change between calls.
  */
 int mtp_compute(mtp_handle* h, int natoms, int nbr_stride, const int* itypes, const double* rijs,
                 const int* js, const int* jtypes, const int* counts, int flags, double* energy,

@@ -35,6 +35,22 @@ struct DeviceSchedule {
   uint2* d_entries = nullptr;
 };
 
+// Arguments of a host-buffer call that a cached CUDA graph replays.  The graph
+// holds the host and device addresses, the sizes and the launch shapes, so it
+// is valid for exactly these and for one generation of the handle's device
+// state (bumped whenever coefficients, launch settings or scratch change).
+struct HostCallKey {
+  int natoms = -1, stride = 0, flags = 0;
+  long long gen = -1;
+  const void* p[8] = {};
+  bool operator==(const HostCallKey& o) const {
+    if (natoms != o.natoms || stride != o.stride || flags != o.flags || gen != o.gen) return false;
+    for (int k = 0; k < 8; ++k)
+      if (p[k] != o.p[k]) return false;
+    return true;
+  }
+};
+
 template <typename T>
 cudaError_t dalloc(T** p, size_t n) {
   *p = nullptr;
@@ -89,6 +105,19 @@ struct mtp_handle {
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> chunk_events;
   int prof_used = 0;
+  // mtp_execute_potential: page-locked staging of the per-atom rows
+  // (allocated on first use, max_atoms x max_nbr)
+  double *hp_rij = nullptr, *hp_F = nullptr;
+  int *hp_js = nullptr, *hp_jt = nullptr, *hp_cnt = nullptr, *hp_types = nullptr;
+  // mtp_compute below kPipelineMinAtoms with page-locked buffers: the call's
+  // copies, kernels and read-backs become one CUDA graph, captured on the
+  // second consecutive call with the same arguments and replayed while they
+  // repeat (a pair style calls with the same buffers every step)
+  long long gen = 0;
+  HostCallKey graph_key, seen_key;
+  cudaGraphExec_t graph_exec = nullptr;
+  bool seen_uncapturable = false;
+  long long graph_captures = 0, graph_replays = 0;
   // statistics
   long long calls = 0;
   double total_ms = 0.0;
@@ -236,6 +265,10 @@ void free_handle(mtp_handle* h) {
   if (h->h_err) cudaFreeHost(h->h_err);
   for (auto ev : h->chunk_events) cudaEventDestroy(ev);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  for (void* q : {static_cast<void*>(h->hp_rij), static_cast<void*>(h->hp_F), static_cast<void*>(h->hp_js),
+                  static_cast<void*>(h->hp_jt), static_cast<void*>(h->hp_cnt), static_cast<void*>(h->hp_types)})
+    if (q) cudaFreeHost(q);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
@@ -312,6 +345,7 @@ int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, 
       h->vscratch_bytes = 0;
       MTP_CUDA(h, cudaMalloc(&h->d_vscratch, need));
       h->vscratch_bytes = need;
+      ++h->gen;
     }
   }
   *ds_out = ds;
@@ -452,15 +486,136 @@ int run_host_pipelined(mtp_handle* h, int natoms, int stride, const int* itypes,
   return st;
 }
 
-int read_err_flags(mtp_handle* h) {
-  MTP_CUDA(h, cudaMemcpyAsync(h->h_err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  MTP_CUDA(h, cudaStreamSynchronize(h->stream));
-  int f = *h->h_err;
+// Status from the device error flags already copied to h_err by finished work
+// (the flags are cleared on the device when set).
+int take_err_flags(mtp_handle* h) {
+  const int f = *h->h_err;
   if (f) MTP_CUDA(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
   if (f & kErrSpecies) return fail(h, MTP_E_SPECIES, "a species index is outside [0, species_count)");
   if (f & kErrCapacity) return fail(h, MTP_E_CAPACITY, "a neighbour count exceeds the row length");
   if (f & kErrNonFinite) return fail(h, MTP_E_NONFINITE, "non-finite energy or force produced on the device");
   return MTP_OK;
+}
+
+int read_err_flags(mtp_handle* h) {
+  MTP_CUDA(h, cudaMemcpyAsync(h->h_err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  MTP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return take_err_flags(h);
+}
+
+// True when [p, p + bytes) is page-locked host memory (cudaHostAlloc or
+// cudaHostRegister): its first and last byte are checked on every call, so a
+// buffer freed and replaced by pageable memory at the same address is seen.
+bool host_pinned(const void* p, size_t bytes) {
+  if (!p || bytes == 0) return true;
+  const char* c = static_cast<const char*>(p);
+  for (const char* q : {c, c + bytes - 1}) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (a.type != cudaMemoryTypeHost) return false;
+  }
+  return true;
+}
+
+// Enqueue one host-buffer call below kPipelineMinAtoms on the handle's stream:
+// input copies, evaluation, totals, and the copies of the results and of the
+// device error flags back to the host.  Nothing here synchronises or
+// allocates, so it can be captured into a graph.
+int enqueue_small_call(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
+                       const int* jtypes, const int* counts, int flags, double* forces, double* eatom,
+                       double* vatom) {
+  const cudaStream_t s = h->stream;
+  const size_t N = natoms, NS = N * stride;
+  if (natoms > 0) {
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_itypes, itypes, N * sizeof(int), cudaMemcpyHostToDevice, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_rijs, rijs, 3 * NS * sizeof(double), cudaMemcpyHostToDevice, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_js, js, NS * sizeof(int), cudaMemcpyHostToDevice, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_jtypes, jtypes, NS * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (counts) MTP_CUDA(h, cudaMemcpyAsync(h->d_counts, counts, N * sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  int st = run_device(h, natoms, stride, h->d_itypes, h->d_rijs, h->d_js, h->d_jtypes, counts ? h->d_counts : nullptr,
+                      true, h->d_F, (flags & MTP_VATOM) ? h->d_vatom : nullptr);
+  if (st != MTP_OK) return st;
+  MTP_CUDA(h, launch_totals(natoms, h->d_E, h->d_wown, h->d_partials, h->d_tot, s));
+  if (natoms > 0) {
+    MTP_CUDA(h, cudaMemcpyAsync(forces, h->d_F, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (flags & MTP_EATOM) MTP_CUDA(h, cudaMemcpyAsync(eatom, h->d_E, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (flags & MTP_VATOM)
+      MTP_CUDA(h, cudaMemcpyAsync(vatom, h->d_vatom, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  MTP_CUDA(h, cudaMemcpyAsync(h->h_tot, h->d_tot, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  MTP_CUDA(h, cudaMemcpyAsync(h->h_err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  return MTP_OK;
+}
+
+// One host-buffer call below kPipelineMinAtoms, synchronous.  With every host
+// buffer page-locked, the second consecutive call with the same arguments is
+// captured into a graph and later ones replay it (one launch instead of about
+// twenty copies and kernels); otherwise the work is enqueued directly.  The
+// results are the same either way: the graph holds the same operations.
+int run_small_call(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
+                   const int* jtypes, const int* counts, int flags, double* forces, double* eatom, double* vatom) {
+  const cudaStream_t s = h->stream;
+  const size_t N = natoms, NS = N * stride;
+  HostCallKey key;
+  key.natoms = natoms;
+  key.stride = stride;
+  key.flags = flags & (MTP_EATOM | MTP_VATOM);
+  key.gen = h->gen;
+  const void* ptrs[8] = {itypes, rijs, js, jtypes, counts, forces,
+                         (flags & MTP_EATOM) ? eatom : nullptr, (flags & MTP_VATOM) ? vatom : nullptr};
+  for (int k = 0; k < 8; ++k) key.p[k] = ptrs[k];
+  const bool pinned = natoms > 0 && !h->profiling && host_pinned(itypes, N * sizeof(int)) &&
+                      host_pinned(rijs, 3 * NS * sizeof(double)) && host_pinned(js, NS * sizeof(int)) &&
+                      host_pinned(jtypes, NS * sizeof(int)) && host_pinned(counts, counts ? N * sizeof(int) : 0) &&
+                      host_pinned(forces, 3 * N * sizeof(double)) &&
+                      host_pinned(key.p[6], (flags & MTP_EATOM) ? N * sizeof(double) : 0) &&
+                      host_pinned(key.p[7], (flags & MTP_VATOM) ? 6 * N * sizeof(double) : 0);
+  bool launched = false;
+  if (pinned && h->graph_exec && key == h->graph_key) {
+    MTP_CUDA(h, cudaGraphLaunch(h->graph_exec, s));
+    launched = true;
+    ++h->graph_replays;
+  } else if (pinned && key == h->seen_key && !h->seen_uncapturable) {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      const int cst = enqueue_small_call(h, natoms, stride, itypes, rijs, js, jtypes, counts, flags, forces, eatom,
+                                         vatom);
+      const cudaError_t ce = cudaStreamEndCapture(s, &g);
+      ok = cst == MTP_OK && ce == cudaSuccess && g != nullptr;
+    }
+    if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    if (ok) {
+      if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+      h->graph_exec = ex;
+      h->graph_key = key;
+      MTP_CUDA(h, cudaGraphLaunch(ex, s));
+      launched = true;
+      ++h->graph_captures;
+    } else {
+      h->seen_uncapturable = true;
+    }
+  } else if (pinned) {
+    h->seen_key = key;
+    h->seen_uncapturable = false;
+  }
+  if (!launched) {
+    const int st = enqueue_small_call(h, natoms, stride, itypes, rijs, js, jtypes, counts, flags, forces, eatom,
+                                      vatom);
+    if (st != MTP_OK) {
+      cudaStreamSynchronize(s);   // copies from the caller's buffers complete before the error returns
+      return st;
+    }
+  }
+  MTP_CUDA(h, cudaStreamSynchronize(s));
+  return take_err_flags(h);
 }
 
 bool ends_with(const std::string& s, const std::string& suf) {
@@ -629,6 +784,15 @@ int mtp_get_info(const mtp_handle* h, int* out8) {
   return MTP_OK;
 }
 
+int mtp_get_stats(const mtp_handle* h, double* out4) {
+  if (!h || !out4) return MTP_E_INVALID;
+  out4[0] = static_cast<double>(h->calls);
+  out4[1] = h->total_ms;
+  out4[2] = static_cast<double>(h->graph_captures);
+  out4[3] = static_cast<double>(h->graph_replays);
+  return MTP_OK;
+}
+
 int mtp_set_coeffs(mtp_handle* h, const double* species, const double* moment, const double* radial) {
   if (!h) return MTP_E_INVALID;
   Potential& p = h->pot;
@@ -636,6 +800,7 @@ int mtp_set_coeffs(mtp_handle* h, const double* species, const double* moment, c
   if (moment) std::copy(moment, moment + p.Sa, p.moment.begin());
   if (radial) std::copy(radial, radial + p.radial.size(), p.radial.begin());
   MTP_CUDA(h, cudaStreamSynchronize(h->stream));
+  ++h->gen;
   return upload_coeffs(h);
 }
 
@@ -648,6 +813,7 @@ int mtp_set_launch(mtp_handle* h, int threads, int bps, int apb) {
   h->threads = threads;
   h->blocks_per_sm = std::max(0, bps);
   h->apb = apb;
+  ++h->gen;
   return MTP_OK;
 }
 
@@ -718,36 +884,26 @@ int mtp_compute(mtp_handle* h, int natoms, int stride, const int* itypes, const 
                                             " neighbours, more than the row length " + std::to_string(stride));
   }
   auto t0 = std::chrono::steady_clock::now();
-  const size_t N = natoms, NS = N * stride;
+  const size_t N = natoms;
   cudaStream_t s = h->stream;
   int st;
   if (natoms >= kPipelineMinAtoms) {
     st = run_host_pipelined(h, natoms, stride, itypes, rijs, js, jtypes, counts,
                             (flags & MTP_VATOM) ? h->d_vatom : nullptr);
-  } else {
-    if (natoms > 0) {
-      MTP_CUDA(h, cudaMemcpyAsync(h->d_itypes, itypes, N * sizeof(int), cudaMemcpyHostToDevice, s));
-      MTP_CUDA(h, cudaMemcpyAsync(h->d_rijs, rijs, 3 * NS * sizeof(double), cudaMemcpyHostToDevice, s));
-      MTP_CUDA(h, cudaMemcpyAsync(h->d_js, js, NS * sizeof(int), cudaMemcpyHostToDevice, s));
-      MTP_CUDA(h, cudaMemcpyAsync(h->d_jtypes, jtypes, NS * sizeof(int), cudaMemcpyHostToDevice, s));
-      if (counts) MTP_CUDA(h, cudaMemcpyAsync(h->d_counts, counts, N * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (st != MTP_OK) {
+      cudaStreamSynchronize(s);   // copies from the caller's buffers complete before the error returns
+      return st;
     }
-    st = run_device(h, natoms, stride, h->d_itypes, h->d_rijs, h->d_js, h->d_jtypes, counts ? h->d_counts : nullptr,
-                    true, h->d_F, (flags & MTP_VATOM) ? h->d_vatom : nullptr);
-  }
-  if (st != MTP_OK) {
-    cudaStreamSynchronize(s);   // copies from the caller's buffers complete before the error returns
-    return st;
-  }
-  MTP_CUDA(h, launch_totals(natoms, h->d_E, h->d_wown, h->d_partials, h->d_tot, s));
-  if (natoms > 0) {
+    MTP_CUDA(h, launch_totals(natoms, h->d_E, h->d_wown, h->d_partials, h->d_tot, s));
     MTP_CUDA(h, cudaMemcpyAsync(forces, h->d_F, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (flags & MTP_EATOM) MTP_CUDA(h, cudaMemcpyAsync(eatom, h->d_E, N * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (flags & MTP_VATOM)
       MTP_CUDA(h, cudaMemcpyAsync(vatom, h->d_vatom, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->h_tot, h->d_tot, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    st = read_err_flags(h);   // synchronises the stream
+  } else {
+    st = run_small_call(h, natoms, stride, itypes, rijs, js, jtypes, counts, flags, forces, eatom, vatom);
   }
-  MTP_CUDA(h, cudaMemcpyAsync(h->h_tot, h->d_tot, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
-  st = read_err_flags(h);   // synchronises the stream
   if (st != MTP_OK) return st;
   if (flags & MTP_EFLAG) *energy = h->h_tot[0];
   if (flags & MTP_VFLAG)
@@ -771,30 +927,57 @@ int mtp_execute_potential(mtp_handle* h, int natoms, int nneigh_total, const dou
                      !forces || !energy || !stress))
     return fail(h, MTP_E_INVALID, "null argument");
   const int stride = h->max_nbr;
-  // pack the per-atom rows into the flat layout (what the reference bridge
-  // copies into its NumPy buffers, zero_overhead.cpp:94-116)
-  std::vector<double> rij(static_cast<size_t>(natoms) * stride * 3, 0.0);
-  std::vector<int> js(static_cast<size_t>(natoms) * stride, -1), jt(static_cast<size_t>(natoms) * stride, -1);
-  std::vector<int> cnt(natoms);
   for (int i = 0; i < natoms; ++i) {
     const int c = neighbor_counts[i];
     if (c < 0 || c > stride)
       return fail(h, MTP_E_CAPACITY, "atom " + std::to_string(i) + " has " + std::to_string(c) +
                                           " neighbours, more than MAX_ATOMS_PER_NEIGHBOR");
-    cnt[i] = c;
-    if (c == 0) continue;
-    std::memcpy(&rij[static_cast<size_t>(i) * stride * 3], atom_positions[i], 3 * c * sizeof(double));
-    std::memcpy(&js[static_cast<size_t>(i) * stride], neighbor_lists[i], c * sizeof(int));
-    std::memcpy(&jt[static_cast<size_t>(i) * stride], neighbor_types_lists[i], c * sizeof(int));
   }
-  std::vector<double> f(3 * static_cast<size_t>(natoms));
+  // persistent page-locked staging (the reference bridge refilled persistent
+  // NumPy buffers, zero_overhead.cpp:61-117): no allocation per step, and the
+  // rows reach the GPU by DMA
+  if (!h->hp_rij) {
+    const size_t rows = static_cast<size_t>(h->max_atoms), slots = rows * stride;
+    void *a = nullptr, *b = nullptr, *c = nullptr, *d = nullptr, *e = nullptr, *f = nullptr;
+    const bool ok = cudaHostAlloc(&a, 3 * slots * sizeof(double), cudaHostAllocDefault) == cudaSuccess &&
+                    cudaHostAlloc(&b, slots * sizeof(int), cudaHostAllocDefault) == cudaSuccess &&
+                    cudaHostAlloc(&c, slots * sizeof(int), cudaHostAllocDefault) == cudaSuccess &&
+                    cudaHostAlloc(&d, std::max<size_t>(rows, 1) * sizeof(int), cudaHostAllocDefault) == cudaSuccess &&
+                    cudaHostAlloc(&e, std::max<size_t>(rows, 1) * sizeof(int), cudaHostAllocDefault) == cudaSuccess &&
+                    cudaHostAlloc(&f, 3 * std::max<size_t>(rows, 1) * sizeof(double), cudaHostAllocDefault) ==
+                        cudaSuccess;
+    if (!ok) {
+      for (void* q : {a, b, c, d, e, f})
+        if (q) cudaFreeHost(q);
+      cudaGetLastError();
+      return fail(h, MTP_E_OOM, "mtp_execute_potential: page-locked staging allocation failed");
+    }
+    h->hp_rij = static_cast<double*>(a);
+    h->hp_js = static_cast<int*>(b);
+    h->hp_jt = static_cast<int*>(c);
+    h->hp_cnt = static_cast<int*>(d);
+    h->hp_types = static_cast<int*>(e);
+    h->hp_F = static_cast<double*>(f);
+  }
+  // pack the counted slots of each row into the flat layout (what the
+  // reference bridge copies into its NumPy buffers, zero_overhead.cpp:94-116);
+  // slots past a row's count are never read
+  for (int i = 0; i < natoms; ++i) {
+    const int c = neighbor_counts[i];
+    h->hp_cnt[i] = c;
+    h->hp_types[i] = atom_types[i];
+    if (c == 0) continue;
+    std::memcpy(h->hp_rij + static_cast<size_t>(i) * stride * 3, atom_positions[i], 3 * c * sizeof(double));
+    std::memcpy(h->hp_js + static_cast<size_t>(i) * stride, neighbor_lists[i], c * sizeof(int));
+    std::memcpy(h->hp_jt + static_cast<size_t>(i) * stride, neighbor_types_lists[i], c * sizeof(int));
+  }
   double vir[6] = {0, 0, 0, 0, 0, 0}, e = 0.0;
-  int st = mtp_compute(h, natoms, stride, atom_types, rij.data(), js.data(), jt.data(), cnt.data(),
-                       MTP_EFLAG | MTP_VFLAG, &e, f.data(), vir, nullptr, nullptr);
+  int st = mtp_compute(h, natoms, stride, h->hp_types, h->hp_rij, h->hp_js, h->hp_jt, h->hp_cnt,
+                       MTP_EFLAG | MTP_VFLAG, &e, h->hp_F, vir, nullptr, nullptr);
   if (st != MTP_OK) return st;
   *energy = e;
   for (int i = 0; i < natoms; ++i)
-    for (int c = 0; c < 3; ++c) forces[i][c] = f[3 * static_cast<size_t>(i) + c];
+    for (int c = 0; c < 3; ++c) forces[i][c] = h->hp_F[3 * static_cast<size_t>(i) + c];
   // reference stress: +sym(sum r g)/V, order xx,yy,zz,yz,xz,xy (jax_backend.py:355-360)
   const double iv = 1.0 / volume;
   stress[0] = -vir[0] * iv;

@@ -33,6 +33,7 @@ SIGNATURES = {
     "mtp_set_stream": (_I, [_P, _P]),
     "mtp_use_own_stream": (_I, [_P]),
     "mtp_get_info": (_I, [_P, _P]),
+    "mtp_get_stats": (_I, [_P, _P]),
     "mtp_set_coeffs": (_I, [_P, _P, _P, _P]),
     "mtp_execute_potential": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _D, _P, _P, _P]),
     "mtp_compute": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P]),

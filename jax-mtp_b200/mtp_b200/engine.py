@@ -107,6 +107,13 @@ class MTPEngine:
     def handle(self):
         return self._h
 
+    def stats(self) -> Dict[str, float]:
+        """Host-buffer call statistics (mtp_get_stats)."""
+        out = np.zeros(4)
+        check(lib().mtp_get_stats(self._h, _ptr(out)), self._h)
+        return {"calls": int(out[0]), "total_ms": float(out[1]), "graph_captures": int(out[2]),
+                "graph_replays": int(out[3])}
+
     def set_coeffs(self, species=None, moment=None, radial=None) -> None:
         sp = None if species is None else _c(species, np.float64)
         mo = None if moment is None else _c(moment, np.float64)

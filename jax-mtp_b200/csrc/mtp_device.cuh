@@ -154,29 +154,29 @@ __device__ __forceinline__ double entry_mult<double>(uint32_t y) {
 }
 
 // Stream one lane program pass: every thread walks its column of the
-// [steps][LANES] entry array with kPrefetch entries in flight (registers), so
-// the L2 latency of the program overlaps the arithmetic.  LANES is a template
-// argument so every request is one load at a constant offset; steps is a
-// multiple of kPrefetch and the program holds kPrefetch rows after any pass,
-// so nothing is bounds-tested.  Each entry feeds A atoms:
+// [steps][LANES] entry array with PF entries in flight (registers), so the L2
+// latency of the program overlaps the arithmetic.  LANES is a template
+// argument so every request is one load at a constant offset; PF divides
+// kStepAlign, so steps is a multiple of PF and the program holds PF rows after
+// any pass: nothing is bounds-tested.  Each entry feeds A atoms:
 // acc[a] += c * V[x][a] * V[y][a]; STORE/ADD flush into V[d][a].
 // Operands are read through Vr and flushes go through V: a pass never reads a
 // slot that it writes, so the two views do not alias.
-template <typename T, int A, int LANES>
+template <typename T, int A, int LANES, int PF>
 __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int steps, int tid, T* __restrict__ V,
                                          const T* __restrict__ Vr) {
-  static_assert(kPrefetch == kStepAlign, "prefetch depth must equal the pass step alignment");
+  static_assert(PF >= 1 && kStepAlign % PF == 0, "prefetch depth must divide the pass step alignment");
   const uint2* p = ent + tid;
-  uint2 buf[kPrefetch];
+  uint2 buf[PF];
 #pragma unroll
-  for (int k = 0; k < kPrefetch; ++k) buf[k] = __ldg(p + k * LANES);
+  for (int k = 0; k < PF; ++k) buf[k] = __ldg(p + k * LANES);
   T acc[A];
 #pragma unroll
   for (int a = 0; a < A; ++a) acc[a] = T(0);
-  for (int s0 = 0; s0 < steps; s0 += kPrefetch) {
-    p += kPrefetch * LANES;
+  for (int s0 = 0; s0 < steps; s0 += PF) {
+    p += PF * LANES;
 #pragma unroll
-    for (int k = 0; k < kPrefetch; ++k) {
+    for (int k = 0; k < PF; ++k) {
       const uint2 e = buf[k];
       buf[k] = __ldg(p + k * LANES);
       const T c = entry_mult<T>(e.y);
@@ -204,28 +204,29 @@ __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int step
 }
 
 // run_pass for the block's lane count (128, 256 or 512 threads).
-template <typename T, int A>
+template <typename T, int A, int PF = kPrefetch>
 __device__ __forceinline__ void run_pass_n(const uint2* __restrict__ ent, int steps, int lanes, int tid,
                                            T* __restrict__ V) {
-  if (lanes == 512) run_pass<T, A, 512>(ent, steps, tid, V, V);
-  else if (lanes == 256) run_pass<T, A, 256>(ent, steps, tid, V, V);
-  else run_pass<T, A, 128>(ent, steps, tid, V, V);
+  if (lanes == 512) run_pass<T, A, 512, PF>(ent, steps, tid, V, V);
+  else if (lanes == 256) run_pass<T, A, 256, PF>(ent, steps, tid, V, V);
+  else run_pass<T, A, 128, PF>(ent, steps, tid, V, V);
 }
 
 // Generic lane-program streamer (used by the dual-number kernels): every thread
-// walks its column of the [steps][LANES] entries with kPrefetch in flight
-// (steps is a multiple of kPrefetch, rows after a pass exist; LANES fixed so
-// every request is one load at a constant offset).
-template <int LANES, typename Body>
+// walks its column of the [steps][LANES] entries with PF in flight.  PF divides
+// kStepAlign, so steps is a multiple of PF and the rows after a pass exist;
+// LANES is fixed so every request is one load at a constant offset.
+template <int LANES, int PF, typename Body>
 __device__ __forceinline__ void stream_entries_t(const uint2* __restrict__ ent, int steps, int tid, Body& body) {
+  static_assert(PF >= 1 && kStepAlign % PF == 0, "prefetch depth must divide the pass step alignment");
   const uint2* p = ent + tid;
-  uint2 buf[kPrefetch];
+  uint2 buf[PF];
 #pragma unroll
-  for (int k = 0; k < kPrefetch; ++k) buf[k] = __ldg(p + k * LANES);
-  for (int s0 = 0; s0 < steps; s0 += kPrefetch) {
-    p += kPrefetch * LANES;
+  for (int k = 0; k < PF; ++k) buf[k] = __ldg(p + k * LANES);
+  for (int s0 = 0; s0 < steps; s0 += PF) {
+    p += PF * LANES;
 #pragma unroll
-    for (int k = 0; k < kPrefetch; ++k) {
+    for (int k = 0; k < PF; ++k) {
       const uint2 e = buf[k];
       buf[k] = __ldg(p + k * LANES);
       body(e);
@@ -233,12 +234,12 @@ __device__ __forceinline__ void stream_entries_t(const uint2* __restrict__ ent, 
   }
 }
 
-template <typename Body>
+template <int PF = kPrefetch, typename Body>
 __device__ __forceinline__ void stream_entries_n(const uint2* __restrict__ ent, int steps, int lanes, int tid,
                                                  Body& body) {
-  if (lanes == 512) stream_entries_t<512>(ent, steps, tid, body);
-  else if (lanes == 256) stream_entries_t<256>(ent, steps, tid, body);
-  else stream_entries_t<128>(ent, steps, tid, body);
+  if (lanes == 512) stream_entries_t<512, PF>(ent, steps, tid, body);
+  else if (lanes == 256) stream_entries_t<256, PF>(ent, steps, tid, body);
+  else stream_entries_t<128, PF>(ent, steps, tid, body);
 }
 
 // Force-phase sums of one or (kTwo) two neighbours over this thread's share

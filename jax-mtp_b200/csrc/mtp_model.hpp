@@ -35,7 +35,7 @@ constexpr int kMaxR = 8;       // radial functions supported by the kernels
 constexpr int kMaxK = 16;      // Chebyshev terms supported by the kernels
 constexpr int kMaxDegree = 12; // monomial degree supported by the kernels
 constexpr int kMaxPasses = 16;
-constexpr int kStepAlign = 8;   // pass steps are a multiple of this; as many no-op rows end the program
+constexpr int kStepAlign = 4;   // pass steps are a multiple of this; as many no-op rows end the program
 
 struct Potential {
   std::string version, potential_name, potential_tag, radial_basis_type;

@@ -80,13 +80,15 @@ def algorithmic_flops(pot, counts_real: np.ndarray) -> float:
     return float(counts_real.sum()) * per_nbr + len(counts_real) * (9 * T + 2 * Sa)
 
 
-def read_traffic():
-    """DRAM bytes per evaluation launch from the committed ncu summary, if any."""
+def read_traffic(threads: int, atoms_per_block: int):
+    """DRAM bytes per evaluation launch from the committed ncu summary, for the
+    launch shape that ran (lines ``traffic_bytes_per_launch_full_workload_t<T>_a<A>:``)."""
     f = os.path.join(ROOT, "profiles", "eval_kernel_l24_mixed.md")
     if not os.path.exists(f):
         return None
+    key = f"traffic_bytes_per_launch_full_workload_t{threads}_a{atoms_per_block}:"
     for line in open(f):
-        if line.startswith("traffic_bytes_per_launch_full_workload:"):
+        if line.startswith(key):
             try:
                 return float(line.split(":", 1)[1].strip())
             except ValueError:
@@ -352,7 +354,8 @@ def run_ours(args):
     k_64 = results["fp64"]["eval_ms_per_launch"] * 1e-3
     achieved = flops / k_mixed / 1e12
     achieved64 = flops / k_64 / 1e12
-    traffic = read_traffic()
+    ran = tuning["mixed"]["ran"]
+    traffic = read_traffic(ran["threads"], ran["atoms_per_block"])
     # the same launch against HBM: algorithmic bytes per atom-step through the
     # evaluation (28 n_pad + 36: r_ij and neighbour index in, force and energy out)
     alg_bytes = (28 * STRIDE + 36) * N

@@ -583,7 +583,10 @@ def run_pair_call(args):
     style calls it: through mtp_compute with page-locked rows (mtp_host_alloc,
     what pair_mtp_b200.cpp packs into) and with pageable numpy arrays, and
     through mtp_execute_potential (the reference bridge's per-atom row pointers,
-    built once outside the timed calls).  Host wall clock per synchronous call."""
+    built once outside the timed calls), and through mtp_compute_positions
+    (page-locked positions of the atoms and their periodic ghosts plus the full
+    neighbour list with a 0.3 A skin, rows built on the GPU).  Host wall clock
+    per synchronous call."""
     import ctypes
     from mtp_b200 import synth
     from mtp_b200._lib import EFLAG, VFLAG, check, lib
@@ -602,6 +605,19 @@ def run_pair_call(args):
     e = np.zeros(1)
     vir = np.zeros(6)
     st = np.zeros(6)
+    # positions + ghosts + neighbour list for the device-rows entry point
+    gx, gown, glists = synth.ghosts_and_lists(s, 5.3)
+    lstride = max(len(c) for c in glists)
+    pos_in = {"x": pinned_empty(gx.shape, np.float64), "sp": pinned_empty((len(gx),), np.int32),
+              "own": pinned_empty((len(gx),), np.int32), "nb": pinned_empty((N, lstride), np.int32),
+              "num": pinned_empty((N,), np.int32)}
+    pos_in["x"][...] = gx
+    pos_in["sp"][...] = s.types[gown]
+    pos_in["own"][...] = gown
+    pos_in["nb"][...] = -1
+    for i, c in enumerate(glists):
+        pos_in["nb"][i, :len(c)] = c
+        pos_in["num"][i] = len(c)
     pinned = {}
     for k, a in (("it", it), ("rij", rij), ("js", js), ("jt", jt), ("cnt", cnt), ("F", F), ("e", e), ("vir", vir)):
         pinned[k] = pinned_empty(a.shape, a.dtype)
@@ -615,7 +631,7 @@ def run_pair_call(args):
     out = {"workload": "level-16 MTP, 2 species, bcc a=2.87 A 10^3 = 2,000 atoms, 60 slots per row, cutoff 5.0 A",
            "calls": calls, "timer": "host wall clock per synchronous call (H2D + kernels + D2H)"}
     for prec in ("fp64", "mixed"):
-        with MTPEngine(path, N, n, precision=prec) as eng:
+        with MTPEngine(path, N, n, cutoff=5.0, precision=prec) as eng:
             h = eng.handle
 
             def flat():
@@ -627,6 +643,12 @@ def run_pair_call(args):
                 check(lib().mtp_compute(h, N, n, P(b["it"]), P(b["rij"]), P(b["js"]), P(b["jt"]), P(b["cnt"]),
                                         EFLAG | VFLAG, P(b["e"]), P(b["F"]), P(b["vir"]), None, None), h)
 
+            def positions():
+                b, q = pinned, pos_in
+                check(lib().mtp_compute_positions(h, N, len(gx), P(q["x"]), P(q["sp"]), P(q["own"]), lstride,
+                                                  P(q["nb"]), P(q["num"]), EFLAG | VFLAG, P(b["e"]), P(b["F"]),
+                                                  P(b["vir"]), None, None), h)
+
             def bridge():
                 check(lib().mtp_execute_potential(h, N, int(cnt.sum()), ctypes.cast(pr, ctypes.c_void_p), P(it),
                                                   ctypes.cast(pj, ctypes.c_void_p), P(cnt),
@@ -634,7 +656,7 @@ def run_pair_call(args):
                                                   ctypes.cast(pf, ctypes.c_void_p), P(st)), h)
 
             for name, fn in (("mtp_compute_pinned", flat_pinned), ("mtp_compute_pageable", flat),
-                             ("mtp_execute_potential", bridge)):
+                             ("mtp_execute_potential", bridge), ("mtp_compute_positions", positions)):
                 for _ in range(5):
                     fn()
                 t0 = time.perf_counter()

@@ -152,6 +152,30 @@ int mtp_compute(mtp_handle* h, int natoms, int nbr_stride, const int* itypes, co
                 double* forces, double* virial, double* eatom, double* vatom);
 
 /*
+ * Host-buffer evaluation from positions: the neighbour rows are built on the
+ * device, so a pair style sends positions and its neighbour list instead of
+ * packed r_ij rows (the host loop of PairJaxMTP::compute,
+ * pair_jax_mtp.cpp:110-167, moves to the GPU).
+ *   x [nall][3]        positions of the nlocal local atoms, then the ghosts
+ *   species [nall]     0-based species of every atom
+ *   owner [nall]       local index of each atom's owner: i for i < nlocal, the
+ *                      local atom with the ghost's tag, or -1 (the ghost then
+ *                      has species -1 in the rows and contributes nothing,
+ *                      pair_jax_mtp.cpp:137-151)
+ *   neigh [nlocal][list_stride]  candidate neighbour indices into [0, nall)
+ *                      (the full list, skin included); numneigh [nlocal]
+ * Candidates closer than the handle's cutoff are kept in list order with
+ * r_ij = x_j - x_i, exactly as a host loop packs them, so the results are
+ * bitwise those of mtp_compute on the rows that loop would build.  More than
+ * max_nbr kept candidates in a row: MTP_E_CAPACITY.  Outputs as mtp_compute;
+ * synchronous.
+ */
+int mtp_compute_positions(mtp_handle* h, int nlocal, int nall, const double* x, const int* species,
+                          const int* owner, int list_stride, const int* neigh, const int* numneigh,
+                          int flags, double* energy, double* forces, double* virial, double* eatom,
+                          double* vatom);
+
+/*
  * Device-pointer variant of mtp_compute for PyTorch and CUDA-graph capture:
  * every pointer is device memory; work is enqueued on the handle's stream and
  * the call returns without synchronising.  energy [1], virial [6].

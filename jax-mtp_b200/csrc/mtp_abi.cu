@@ -118,6 +118,11 @@ struct mtp_handle {
   cudaGraphExec_t graph_exec = nullptr;
   bool seen_uncapturable = false;
   long long graph_captures = 0, graph_replays = 0;
+  // mtp_compute_positions: positions, species and owners of local and ghost
+  // atoms [all_cap], candidate lists [neigh_cap], list lengths [max_atoms]
+  double* d_xall = nullptr;
+  int *d_spall = nullptr, *d_owner = nullptr, *d_neigh = nullptr, *d_numneigh = nullptr;
+  size_t all_cap = 0, neigh_cap = 0;
   // statistics
   long long calls = 0;
   double total_ms = 0.0;
@@ -254,6 +259,7 @@ void free_handle(mtp_handle* h) {
   F(h->d_G); F(h->d_E); F(h->d_F); F(h->d_wown); F(h->d_vatom);
   F(h->d_in_cnt); F(h->d_in_ptr); F(h->d_in_cursor); F(h->d_in_slot); F(h->d_blk);
   F(h->d_partials); F(h->d_tot); F(h->d_err); F(h->d_cfg_ptr); F(h->d_vscratch);
+  F(h->d_xall); F(h->d_spall); F(h->d_owner); F(h->d_neigh); F(h->d_numneigh);
   train_free(h->train);
   F(h->cells.cell); F(h->cells.img); F(h->cells.cnt); F(h->cells.ptr); F(h->cells.cursor); F(h->cells.atoms);
   F(h->cells.blk);
@@ -912,6 +918,81 @@ int mtp_compute(mtp_handle* h, int natoms, int stride, const int* itypes, const 
   double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   h->total_ms += ms;
   if (h->debug >= 2) std::fprintf(stderr, "[mtp_b200] call %lld: natoms=%d %.3f ms\n", h->calls, natoms, ms);
+  return MTP_OK;
+}
+
+int mtp_compute_positions(mtp_handle* h, int nlocal, int nall, const double* x, const int* species, const int* owner,
+                          int list_stride, const int* neigh, const int* numneigh, int flags, double* energy,
+                          double* forces, double* virial, double* eatom, double* vatom) {
+  if (!h) return MTP_E_INVALID;
+  if (nlocal < 0 || nall < nlocal || list_stride < 0)
+    return fail(h, MTP_E_INVALID, "need 0 <= nlocal <= nall and list_stride >= 0");
+  if (nlocal > h->max_atoms)
+    return fail(h, MTP_E_CAPACITY, "nlocal " + std::to_string(nlocal) + " exceeds max_atoms " +
+                                        std::to_string(h->max_atoms));
+  if (nlocal > 0 && (list_stride == 0 || !x || !species || !owner || !neigh || !numneigh || !forces))
+    return fail(h, MTP_E_INVALID, "null input or forces pointer, or list_stride 0 with atoms");
+  if ((flags & MTP_EFLAG) && !energy) return fail(h, MTP_E_INVALID, "MTP_EFLAG without an energy pointer");
+  if ((flags & MTP_VFLAG) && !virial) return fail(h, MTP_E_INVALID, "MTP_VFLAG without a virial pointer");
+  if ((flags & MTP_EATOM) && !eatom) return fail(h, MTP_E_INVALID, "MTP_EATOM without an eatom pointer");
+  if ((flags & MTP_VATOM) && !vatom) return fail(h, MTP_E_INVALID, "MTP_VATOM without a vatom pointer");
+  auto t0 = std::chrono::steady_clock::now();
+  const cudaStream_t s = h->stream;
+  const size_t N = nlocal, NA = nall, NN = N * list_stride;
+  if (NA > h->all_cap) {
+    MTP_CUDA(h, cudaStreamSynchronize(s));
+    cudaFree(h->d_xall);
+    cudaFree(h->d_spall);
+    cudaFree(h->d_owner);
+    h->d_xall = nullptr;
+    h->d_spall = h->d_owner = nullptr;
+    h->all_cap = 0;
+    MTP_CUDA(h, dalloc(&h->d_xall, 3 * NA));
+    MTP_CUDA(h, dalloc(&h->d_spall, NA));
+    MTP_CUDA(h, dalloc(&h->d_owner, NA));
+    h->all_cap = NA;
+  }
+  if (NN > h->neigh_cap) {
+    MTP_CUDA(h, cudaStreamSynchronize(s));
+    cudaFree(h->d_neigh);
+    h->d_neigh = nullptr;
+    h->neigh_cap = 0;
+    MTP_CUDA(h, dalloc(&h->d_neigh, NN));
+    h->neigh_cap = NN;
+  }
+  if (!h->d_numneigh) MTP_CUDA(h, dalloc(&h->d_numneigh, static_cast<size_t>(h->max_atoms)));
+  const int stride = h->max_nbr;
+  if (nlocal > 0) {
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_xall, x, 3 * NA * sizeof(double), cudaMemcpyHostToDevice, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_spall, species, NA * sizeof(int), cudaMemcpyHostToDevice, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_owner, owner, NA * sizeof(int), cudaMemcpyHostToDevice, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_neigh, neigh, NN * sizeof(int), cudaMemcpyHostToDevice, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->d_numneigh, numneigh, N * sizeof(int), cudaMemcpyHostToDevice, s));
+    MTP_CUDA(h, launch_rows_from_positions(nlocal, nall, h->d_xall, h->d_spall, h->d_owner, list_stride, h->d_neigh,
+                                           h->d_numneigh, h->cutoff, stride, h->d_rijs, h->d_js, h->d_jtypes,
+                                           h->d_counts, h->d_err, s));
+  }
+  int st = run_device(h, nlocal, stride, nlocal > 0 ? h->d_spall : h->d_itypes, h->d_rijs, h->d_js, h->d_jtypes,
+                      h->d_counts, true, h->d_F, (flags & MTP_VATOM) ? h->d_vatom : nullptr);
+  if (st != MTP_OK) {
+    cudaStreamSynchronize(s);   // copies from the caller's buffers complete before the error returns
+    return st;
+  }
+  MTP_CUDA(h, launch_totals(nlocal, h->d_E, h->d_wown, h->d_partials, h->d_tot, s));
+  if (nlocal > 0) {
+    MTP_CUDA(h, cudaMemcpyAsync(forces, h->d_F, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (flags & MTP_EATOM) MTP_CUDA(h, cudaMemcpyAsync(eatom, h->d_E, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (flags & MTP_VATOM)
+      MTP_CUDA(h, cudaMemcpyAsync(vatom, h->d_vatom, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  MTP_CUDA(h, cudaMemcpyAsync(h->h_tot, h->d_tot, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  st = read_err_flags(h);   // synchronises the stream
+  if (st != MTP_OK) return st;
+  if (flags & MTP_EFLAG) *energy = h->h_tot[0];
+  if (flags & MTP_VFLAG)
+    for (int c = 0; c < 6; ++c) virial[c] = h->h_tot[1 + c];
+  h->calls++;
+  h->total_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return MTP_OK;
 }
 

@@ -373,6 +373,74 @@ __global__ void k_final_totals(int nb, const double* __restrict__ partials, doub
   }
 }
 
+// Neighbour rows from positions, one warp per local atom: the candidates of
+// the atom's list closer than the cutoff are kept in list order (a ballot and
+// a prefix count give each kept candidate its slot), with r_ij = x_j - x_i,
+// the owner index of j and its species (-1 for a ghost without an owner).
+// This is the host packing loop of the pair style (pair_jax_mtp.cpp:110-167)
+// on the device: r^2 is formed with separately rounded products and sums, as
+// that loop does, so the same candidates are kept.
+__global__ void k_rows_from_positions(int nlocal, int nall, const double* __restrict__ x,
+                                      const int* __restrict__ species, const int* __restrict__ owner,
+                                      int list_stride, const int* __restrict__ neigh,
+                                      const int* __restrict__ numneigh, double cut2, int stride,
+                                      double* __restrict__ rijs, int* __restrict__ js, int* __restrict__ jtypes,
+                                      int* __restrict__ counts, int* __restrict__ err) {
+  const int i = static_cast<int>((static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= nlocal) return;   // the warp leaves together
+  const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
+  const int n = min(max(numneigh[i], 0), list_stride);
+  const int* row = neigh + static_cast<size_t>(i) * list_stride;
+  int kept = 0;
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    const int c = c0 + lane;
+    bool keep = false;
+    double dx = 0.0, dy = 0.0, dz = 0.0;
+    int j = -1;
+    if (c < n) {
+      j = row[c];
+      if (j >= 0 && j < nall && j != i) {
+        dx = x[3 * j] - xi;
+        dy = x[3 * j + 1] - yi;
+        dz = x[3 * j + 2] - zi;
+        const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        keep = r2 < cut2;
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      const int slot = kept + __popc(m & ((1u << lane) - 1u));
+      if (slot < stride) {
+        const size_t o = static_cast<size_t>(i) * stride + slot;
+        rijs[3 * o] = dx;
+        rijs[3 * o + 1] = dy;
+        rijs[3 * o + 2] = dz;
+        const int own = owner[j];
+        js[o] = own;
+        jtypes[o] = own >= 0 ? species[j] : -1;
+      }
+    }
+    kept += __popc(m);
+  }
+  if (lane == 0) {
+    counts[i] = min(kept, stride);
+    if (kept > stride) atomicOr(err, kErrCapacity);
+  }
+}
+
+cudaError_t launch_rows_from_positions(int nlocal, int nall, const double* x, const int* species, const int* owner,
+                                       int list_stride, const int* neigh, const int* numneigh, double cutoff,
+                                       int stride, double* rijs, int* js, int* jtypes, int* counts, int* err,
+                                       cudaStream_t st) {
+  if (nlocal <= 0) return cudaSuccess;
+  const size_t threads = static_cast<size_t>(nlocal) * 32;
+  k_rows_from_positions<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, st>>>(
+      nlocal, nall, x, species, owner, list_stride, neigh, numneigh, cutoff * cutoff, stride, rijs, js, jtypes,
+      counts, err);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_totals(int natoms, const double* site_energy, const double* wown, double* partials,
                           double* out, cudaStream_t st) {
   if (natoms <= 0) {

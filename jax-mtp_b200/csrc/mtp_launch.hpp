@@ -44,6 +44,14 @@ cudaError_t launch_config_totals(int natoms, int nconfig, const int* cfg_ptr, co
 cudaError_t launch_config_ptr(int natoms, int nconfig, const int* cfg_of_atom, int* cfg_ptr, int* err,
                               cudaStream_t st);
 
+// Rows [nlocal][stride] (r_ij, owner index, species, count) from positions
+// x [nall][3] and candidate lists neigh [nlocal][list_stride]: candidates
+// closer than cutoff, in list order; more than stride sets kErrCapacity.
+cudaError_t launch_rows_from_positions(int nlocal, int nall, const double* x, const int* species, const int* owner,
+                                       int list_stride, const int* neigh, const int* numneigh, double cutoff,
+                                       int stride, double* rijs, int* js, int* jtypes, int* counts, int* err,
+                                       cudaStream_t st);
+
 // FMA-chain peak probe.
 cudaError_t measure_fma_peak(double* fp64_tflops, double* fp32_tflops);
 

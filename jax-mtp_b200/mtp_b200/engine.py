@@ -166,6 +166,35 @@ class MTPEngine:
             out["vatom"] = va
         return out
 
+    def compute_positions(self, nlocal: int, x, species, owner, neigh, numneigh, eatom: bool = True,
+                          vatom: bool = False):
+        """Host arrays in, rows built on the device (mtp_compute_positions):
+        x [nall, 3] local atoms then ghosts, species [nall] (0-based), owner
+        [nall] (local owner index or -1), neigh [nlocal, list_stride] candidate
+        indices into [0, nall), numneigh [nlocal].  Returns what ``compute`` returns."""
+        xa = _c(x, np.float64)
+        sp = _c(species, np.int32)
+        ow = _c(owner, np.int32)
+        nb = _c(neigh, np.int32)
+        nn = _c(numneigh, np.int32)
+        nall = int(sp.shape[0])
+        stride = int(nb.shape[1]) if nb.ndim == 2 else 0
+        F = np.zeros((nlocal, 3))
+        vir = np.zeros(6)
+        e = np.zeros(1)
+        ea = np.zeros(nlocal) if eatom else None
+        va = np.zeros((nlocal, 6)) if vatom else None
+        flags = EFLAG | VFLAG | (EATOM if eatom else 0) | (VATOM if vatom else 0)
+        code = lib().mtp_compute_positions(self._h, nlocal, nall, _ptr(xa), _ptr(sp), _ptr(ow), stride, _ptr(nb),
+                                           _ptr(nn), flags, _ptr(e), _ptr(F), _ptr(vir), _ptr(ea), _ptr(va))
+        check(code, self._h)
+        out = {"energy": float(e[0]), "forces": F, "virial": vir}
+        if eatom:
+            out["site_energies"] = ea
+        if vatom:
+            out["vatom"] = va
+        return out
+
     def execute_potential(self, itypes, rijs, js, jtypes, counts, volume: float):
         """The reference bridge signature (zero_overhead.hpp:58-64): per-atom row
         pointers in, (ok, energy, forces [N,3], stress [6] in the reference's

@@ -108,6 +108,41 @@ def _image_ranges(cell: np.ndarray, cutoff: float) -> np.ndarray:
     return np.array(out)
 
 
+def ghosts_and_lists(s: Structure, rlist: float):
+    """Local atoms, periodic ghosts and full neighbour lists as an MD code hands
+    them to a pair style (orthorhombic cells whose edges exceed ``rlist``).
+
+    Returns (x [nall, 3] wrapped local positions then ghost images within
+    ``rlist`` of the box, owner [nall] int32 local index of each atom's owner,
+    lists: for every local atom the indices of all other atoms closer than
+    ``rlist``, in index order).
+    """
+    cell = np.asarray(s.cell, dtype=np.float64)
+    if np.count_nonzero(cell - np.diag(np.diag(cell))) or np.any(np.diag(cell) <= rlist):
+        raise ValueError("ghosts_and_lists needs an orthorhombic cell with edges longer than rlist")
+    L = np.diag(cell).copy()
+    N = s.natoms
+    pos = np.mod(s.positions, L)
+    xs, own = [pos], [np.arange(N)]
+    for sx in (-1, 0, 1):
+        for sy in (-1, 0, 1):
+            for sz in (-1, 0, 1):
+                if sx == sy == sz == 0:
+                    continue
+                img = pos + np.array([sx, sy, sz]) * L
+                keep = np.all((img > -rlist) & (img < L + rlist), axis=1)
+                xs.append(img[keep])
+                own.append(np.arange(N)[keep])
+    x = np.concatenate(xs)
+    owner = np.concatenate(own).astype(np.int32)
+    idx = np.arange(len(x))
+    lists = []
+    for i in range(N):
+        d2 = np.sum((x - x[i]) ** 2, axis=1)
+        lists.append(np.nonzero((d2 < rlist * rlist) & (idx != i))[0].astype(np.int32))
+    return x, owner, lists
+
+
 def build_neighbors(s: Structure, cutoff: float, n_pad: Optional[int] = None,
                     pad_multiple: int = 8) -> NeighborData:
     """Full neighbour list with every periodic image inside ``cutoff``.

@@ -155,7 +155,7 @@ void build_list(Sim& s, double rcut) {
 int main(int argc, char** argv) {
   if (argc < 11) {
     std::fprintf(stderr, "usage: %s data.txt potential.mtp max_atoms max_nbr cutoff mass dt steps every skin "
-                         "[fp64|mixed] [thermo_every]\n", argv[0]);
+                         "[fp64|mixed] [thermo_every] [device|host rows]\n", argv[0]);
     return 2;
   }
   const std::string data = argv[1], pot = argv[2];
@@ -165,6 +165,7 @@ int main(int argc, char** argv) {
   const double skin = std::atof(argv[10]);
   const std::string prec = argc > 11 ? argv[11] : "fp64";
   const int thermo = argc > 12 ? std::atoi(argv[12]) : 100;
+  const std::string rows = argc > 13 ? argv[13] : "device";
 
   Sim s;
   {
@@ -201,8 +202,9 @@ int main(int argc, char** argv) {
   try {
     PairMTPB200 pair(&lmp);
     std::string a1 = pot, a2 = std::to_string(max_atoms), a3 = std::to_string(max_nbr), a4 = argv[5], a5 = "0";
-    char* sargs[] = {&a1[0], &a2[0], &a3[0], &a4[0], &a5[0], const_cast<char*>(prec.c_str())};
-    pair.settings(6, sargs);
+    std::string a7 = "rows", a8 = rows;
+    char* sargs[] = {&a1[0], &a2[0], &a3[0], &a4[0], &a5[0], const_cast<char*>(prec.c_str()), &a7[0], &a8[0]};
+    pair.settings(8, sargs);
     char star[] = "*";
     char* cargs[] = {star, star};
     pair.coeff(2, cargs);

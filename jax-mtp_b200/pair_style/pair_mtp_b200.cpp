@@ -3,13 +3,16 @@
 
    Per step (compare PairJaxMTP::compute, pair_jax_mtp.cpp:69-207):
      - for every local atom i of the full list, neighbours j with
-       |x_j - x_i| < MTP_CUTOFF go to row i of persistent flat buffers:
-       r_ij = x_j - x_i (the ghost coordinates already hold the periodic
-       image), the owner's local index, the owner's species (type - 1);
-       a ghost without a local owner gets species -1 and is skipped by the
-       evaluator, as in the reference (pair_jax_mtp.cpp:137-151);
-     - one mtp_compute call (energy, forces with the reaction terms folded
-       onto owners, virial, optional per-atom energy/virial);
+       |x_j - x_i| < MTP_CUTOFF form row i: r_ij = x_j - x_i (the ghost
+       coordinates already hold the periodic image), the owner's local
+       index, the owner's species (type - 1); a ghost without a local owner
+       gets species -1 and is skipped by the evaluator, as in the reference
+       (pair_jax_mtp.cpp:137-151).  With rows device (the default) the GPU
+       builds the rows from positions and the list (mtp_compute_positions);
+       with rows host they are packed here into persistent page-locked
+       buffers (mtp_compute);
+     - one call (energy, forces with the reaction terms folded onto owners,
+       virial, optional per-atom energy/virial);
      - f[i] += F_i, eng_vdwl += E, virial += W (LAMMPS convention).
    Differences from the reference, each a fix: a row longer than
    MAX_ATOMS_PER_NEIGHBOR and nlocal > MAX_ATOMS are errors instead of silent
@@ -47,6 +50,7 @@ PairMTPB200::PairMTPB200(LAMMPS *lmp) : Pair(lmp)
   max_atoms = max_nbr = 0;
   debug_level = 0;
   precision = MTP_PRECISION_FP64;
+  rows_on_device = 1;
   handle = nullptr;
   total_calls = 0;
 }
@@ -93,49 +97,83 @@ void PairMTPB200::compute(int eflag, int vflag)
   for (int i = 0; i < nlocal; ++i) maxtag = tag[i] > maxtag ? tag[i] : maxtag;
   tag_to_local.assign(static_cast<size_t>(maxtag) + 1, -1);
   for (int i = 0; i < nlocal; ++i) tag_to_local[tag[i]] = i;
+  auto owner_of = [&](int j) {
+    if (j < nlocal) return j;
+    return (tag[j] >= 0 && tag[j] <= maxtag) ? tag_to_local[tag[j]] : -1;
+  };
 
   const int inum = list->inum;
   const int *ilist = list->ilist;
   const int *numneigh = list->numneigh;
   int **firstneigh = list->firstneigh;
-  const double rc2 = cutoff * cutoff;
-
-  std::memset(counts.data(), 0, sizeof(int) * nlocal);
-  for (int i = 0; i < nlocal; ++i) itypes[i] = type[i] - 1;
-  for (int ii = 0; ii < inum; ++ii) {
-    const int i = ilist[ii];
-    const double xi = x[i][0], yi = x[i][1], zi = x[i][2];
-    const int *jlist = firstneigh[i];
-    const size_t row = static_cast<size_t>(i) * max_nbr;
-    int n = 0;
-    for (int jj = 0; jj < numneigh[i]; ++jj) {
-      const int j = jlist[jj] & NEIGHMASK;
-      if (j == i || j >= nall) continue;
-      const double dx = x[j][0] - xi, dy = x[j][1] - yi, dz = x[j][2] - zi;
-      if (dx * dx + dy * dy + dz * dz >= rc2) continue;
-      if (n == max_nbr)
-        error->one(FLERR, "pair jax/mtp: atom " + std::to_string(tag[i]) +
-                              " has more neighbours than MAX_ATOMS_PER_NEIGHBOR " + std::to_string(max_nbr));
-      int owner = j;
-      if (j >= nlocal) owner = (tag[j] >= 0 && tag[j] <= maxtag) ? tag_to_local[tag[j]] : -1;
-      double *r = &rij[3 * (row + n)];
-      r[0] = dx;
-      r[1] = dy;
-      r[2] = dz;
-      js[row + n] = owner;
-      jtypes[row + n] = owner >= 0 ? type[j] - 1 : -1;
-      ++n;
-    }
-    counts[i] = n;
-  }
 
   int flags = MTP_EFLAG | MTP_VFLAG;
   if (eflag_atom) flags |= MTP_EATOM;
   if (vflag_atom) flags |= MTP_VATOM;
   double energy = 0.0, w[6] = {0, 0, 0, 0, 0, 0};
-  const int status =
-      mtp_compute(handle, nlocal, max_nbr, itypes.data(), rij.data(), js.data(), jtypes.data(), counts.data(), flags,
-                  &energy, fbuf.data(), w, eflag_atom ? ebuf.data() : nullptr, vflag_atom ? vbuf.data() : nullptr);
+  int status;
+  if (rows_on_device) {
+    // positions, species and owners of every atom, and the neighbour list as
+    // it is (skin included): the GPU keeps the candidates inside the cutoff
+    // (mtp_compute_positions)
+    int lstride = 1;
+    for (int ii = 0; ii < inum; ++ii) lstride = numneigh[ilist[ii]] > lstride ? numneigh[ilist[ii]] : lstride;
+    const size_t na = static_cast<size_t>(nall);
+    if (!(xall.ensure(3 * na) && spall.ensure(na) && owner.ensure(na) &&
+          neigh.ensure(static_cast<size_t>(nlocal) * lstride) && nneigh.ensure(static_cast<size_t>(nlocal) + 1)))
+      error->one(FLERR, std::string("pair jax/mtp: page-locked buffers: ") + mtp_last_error(nullptr));
+    for (int j = 0; j < nall; ++j) {
+      xall[3 * j] = x[j][0];
+      xall[3 * j + 1] = x[j][1];
+      xall[3 * j + 2] = x[j][2];
+      spall[j] = type[j] - 1;
+      owner[j] = owner_of(j);
+    }
+    std::memset(nneigh.data(), 0, sizeof(int) * nlocal);
+    for (int ii = 0; ii < inum; ++ii) {
+      const int i = ilist[ii];
+      const int *jlist = firstneigh[i];
+      int *row = neigh.data() + static_cast<size_t>(i) * lstride;
+      for (int jj = 0; jj < numneigh[i]; ++jj) row[jj] = jlist[jj] & NEIGHMASK;
+      nneigh[i] = numneigh[i];
+    }
+    status = mtp_compute_positions(handle, nlocal, nall, xall.data(), spall.data(), owner.data(), lstride,
+                                   neigh.data(), nneigh.data(), flags, &energy, fbuf.data(), w,
+                                   eflag_atom ? ebuf.data() : nullptr, vflag_atom ? vbuf.data() : nullptr);
+  } else {
+    // rows packed on the host, as the reference pair style does
+    const double rc2 = cutoff * cutoff;
+    std::memset(counts.data(), 0, sizeof(int) * nlocal);
+    for (int i = 0; i < nlocal; ++i) itypes[i] = type[i] - 1;
+    for (int ii = 0; ii < inum; ++ii) {
+      const int i = ilist[ii];
+      const double xi = x[i][0], yi = x[i][1], zi = x[i][2];
+      const int *jlist = firstneigh[i];
+      const size_t row = static_cast<size_t>(i) * max_nbr;
+      int n = 0;
+      for (int jj = 0; jj < numneigh[i]; ++jj) {
+        const int j = jlist[jj] & NEIGHMASK;
+        if (j == i || j >= nall) continue;
+        const double dx = x[j][0] - xi, dy = x[j][1] - yi, dz = x[j][2] - zi;
+        if (dx * dx + dy * dy + dz * dz >= rc2) continue;
+        if (n == max_nbr)
+          error->one(FLERR, "pair jax/mtp: atom " + std::to_string(tag[i]) +
+                                " has more neighbours than MAX_ATOMS_PER_NEIGHBOR " + std::to_string(max_nbr));
+        const int own = owner_of(j);
+        double *r = &rij[3 * (row + n)];
+        r[0] = dx;
+        r[1] = dy;
+        r[2] = dz;
+        js[row + n] = own;
+        jtypes[row + n] = own >= 0 ? type[j] - 1 : -1;
+        ++n;
+      }
+      counts[i] = n;
+    }
+    status = mtp_compute(handle, nlocal, max_nbr, itypes.data(), rij.data(), js.data(), jtypes.data(), counts.data(),
+                         flags, &energy, fbuf.data(), w, eflag_atom ? ebuf.data() : nullptr,
+                         vflag_atom ? vbuf.data() : nullptr);
+  }
   if (status != MTP_OK) error->one(FLERR, std::string("pair jax/mtp: ") + mtp_last_error(handle));
 
   for (int i = 0; i < nlocal; ++i) {
@@ -156,9 +194,16 @@ void PairMTPB200::compute(int eflag, int vflag)
 
 void PairMTPB200::settings(int narg, char **arg)
 {
+  // trailing "rows device|host" keyword
+  if (narg >= 6 && strcmp(arg[narg - 2], "rows") == 0) {
+    if (strcmp(arg[narg - 1], "device") == 0) rows_on_device = 1;
+    else if (strcmp(arg[narg - 1], "host") == 0) rows_on_device = 0;
+    else error->all(FLERR, "pair jax/mtp: rows must be device or host");
+    narg -= 2;
+  }
   if (narg < 4 || narg > 6)
     error->all(FLERR, "Illegal pair_style command: pair_style jax/mtp <potential.mtp> <max_atoms> "
-                      "<max_neighbors> <cutoff> [debug_level] [fp64|mixed]");
+                      "<max_neighbors> <cutoff> [debug_level] [fp64|mixed] [rows device|host]");
   delete[] mtp_path;
   mtp_path = new char[strlen(arg[0]) + 1];
   strcpy(mtp_path, arg[0]);

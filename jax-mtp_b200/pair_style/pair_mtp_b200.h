@@ -5,11 +5,15 @@
    pair_jax_mtp.cpp:228-282):
 
      pair_style jax/mtp <potential.mtp> MAX_ATOMS MAX_ATOMS_PER_NEIGHBOR MTP_CUTOFF [DEBUG_LEVEL] [fp64|mixed]
+                        [rows device|host]
      pair_coeff * *
 
    The first argument is the .mtp potential itself (the reference took a
    jax.export .bin compiled from it; a .bin is rejected with a clear error).
    Needs atom IDs, a full neighbour list, and one MPI rank (as the reference).
+   rows device (the default) sends positions and the neighbour list and lets
+   the GPU build the rows (mtp_compute_positions); rows host packs r_ij on
+   the host as the reference did (mtp_compute).  Both give the same results.
 ------------------------------------------------------------------------- */
 
 #ifdef PAIR_CLASS
@@ -53,6 +57,19 @@ template <typename T> class PinnedArray {
     for (size_t i = 0; i < n_; ++i) p_[i] = v;
     return true;
   }
+  // at least n elements (contents kept only when nothing is reallocated)
+  bool ensure(size_t n)
+  {
+    if (n <= n_) return true;
+    mtp_host_free(p_);
+    p_ = nullptr;
+    n_ = 0;
+    void *q = nullptr;
+    if (mtp_host_alloc(n * sizeof(T), &q) != MTP_OK) return false;
+    p_ = static_cast<T *>(q);
+    n_ = n;
+    return true;
+  }
   size_t size() const { return n_; }
   T *data() { return p_; }
   T &operator[](size_t i) { return p_[i]; }
@@ -83,6 +100,7 @@ class PairMTPB200 : public Pair {
   char *mtp_path;
   double cutoff;
   int max_atoms, max_nbr, debug_level, precision;
+  int rows_on_device;
   mtp_handle *handle;
   long long total_calls;
 
@@ -92,6 +110,10 @@ class PairMTPB200 : public Pair {
   PinnedArray<int> js, jtypes, counts, itypes;
   PinnedArray<double> fbuf, ebuf, vbuf;
   std::vector<int> tag_to_local;
+  // rows device: positions, species and owners of local + ghost atoms, and
+  // the neighbour list [nlocal][list stride], page-locked
+  PinnedArray<double> xall;
+  PinnedArray<int> spall, owner, neigh, nneigh;
 };
 
 }    // namespace LAMMPS_NS

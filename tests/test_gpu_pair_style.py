@@ -31,11 +31,11 @@ def driver():
     return DRIVER
 
 
-def _run(driver, tmp_path, s, v, pot_name, steps, precision="fp64", thermo=10):
+def _run(driver, tmp_path, s, v, pot_name, steps, precision="fp64", thermo=10, rows="device"):
     data = tmp_path / "data.txt"
     write_data(str(data), s, v, 2)
     out = subprocess.run([driver, str(data), potential_path(pot_name), str(s.natoms), "64", "5.0", "55.845",
-                          "0.001", str(steps), "10", "0.3", precision, str(thermo)],
+                          "0.001", str(steps), "10", "0.3", precision, str(thermo), rows],
                          capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr
     lines = out.stdout.strip().splitlines()
@@ -67,3 +67,17 @@ def test_pair_style_nve_config1(driver, tmp_path):
     # mixed vs FP64 potential energy at step 0 (meV/atom)
     de = abs(float(th2[0][1]) - float(th[0][1])) / s.natoms * 1e3
     assert de < 0.1, de
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_pair_style_device_rows_match_host_rows(driver, tmp_path, precision):
+    """rows device (positions + list to the GPU) and rows host (r_ij packed on
+    the host) give the same trajectory, thermo line for thermo line."""
+    s = synth.lattice_structure("bcc", 2.87, (5, 5, 5))
+    s.positions += np.random.default_rng(5).normal(0, 0.05, s.positions.shape)
+    s.types = np.random.default_rng(6).integers(0, 2, s.natoms).astype(np.int32)
+    v = np.random.default_rng(7).normal(0, 0.02, (s.natoms, 3))
+    dev, _ = _run(driver, tmp_path, s, v, "cfg1md_L16_S2.mtp", 30, precision, 5, "device")
+    host, _ = _run(driver, tmp_path, s, v, "cfg1md_L16_S2.mtp", 30, precision, 5, "host")
+    assert len(dev) == len(host) == 7
+    assert dev == host

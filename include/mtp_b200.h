@@ -168,7 +168,9 @@ int mtp_compute(mtp_handle* h, int natoms, int nbr_stride, const int* itypes, co
  * r_ij = x_j - x_i, exactly as a host loop packs them, so the results are
  * bitwise those of mtp_compute on the rows that loop would build.  More than
  * max_nbr kept candidates in a row: MTP_E_CAPACITY.  Outputs as mtp_compute;
- * synchronous.
+ * synchronous.  With every buffer page-locked and the handle on a non-default
+ * stream, the second consecutive call with the same arguments is captured as
+ * one CUDA graph and replayed while they repeat, as for mtp_compute.
  */
 int mtp_compute_positions(mtp_handle* h, int nlocal, int nall, const double* x, const int* species,
                           const int* owner, int list_stride, const int* neigh, const int* numneigh,

@@ -40,11 +40,14 @@ struct DeviceSchedule {
 // is valid for exactly these and for one generation of the handle's device
 // state (bumped whenever coefficients, launch settings or scratch change).
 struct HostCallKey {
-  int natoms = -1, stride = 0, flags = 0;
+  int kind = -1;   // 0: mtp_compute, 1: mtp_compute_positions
+  int natoms = -1, stride = 0, flags = 0, extra = 0;
   long long gen = -1;
   const void* p[8] = {};
   bool operator==(const HostCallKey& o) const {
-    if (natoms != o.natoms || stride != o.stride || flags != o.flags || gen != o.gen) return false;
+    if (kind != o.kind || natoms != o.natoms || stride != o.stride || flags != o.flags || extra != o.extra ||
+        gen != o.gen)
+      return false;
     for (int k = 0; k < 8; ++k)
       if (p[k] != o.p[k]) return false;
     return true;
@@ -557,29 +560,14 @@ int enqueue_small_call(mtp_handle* h, int natoms, int stride, const int* itypes,
   return MTP_OK;
 }
 
-// One host-buffer call below kPipelineMinAtoms, synchronous.  With every host
-// buffer page-locked, the second consecutive call with the same arguments is
-// captured into a graph and later ones replay it (one launch instead of about
-// twenty copies and kernels); otherwise the work is enqueued directly.  The
-// results are the same either way: the graph holds the same operations.
-int run_small_call(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
-                   const int* jtypes, const int* counts, int flags, double* forces, double* eatom, double* vatom) {
+// Run one synchronous host-buffer call.  With every host buffer page-locked
+// (pinned), the second consecutive call with the same key is captured into a
+// graph and later ones replay it (one launch instead of about twenty copies
+// and kernels); otherwise enqueue() runs directly.  The results are the same
+// either way: the graph holds the same operations.
+template <typename Enqueue>
+int run_graphable(mtp_handle* h, const HostCallKey& key, bool pinned, Enqueue&& enqueue) {
   const cudaStream_t s = h->stream;
-  const size_t N = natoms, NS = N * stride;
-  HostCallKey key;
-  key.natoms = natoms;
-  key.stride = stride;
-  key.flags = flags & (MTP_EATOM | MTP_VATOM);
-  key.gen = h->gen;
-  const void* ptrs[8] = {itypes, rijs, js, jtypes, counts, forces,
-                         (flags & MTP_EATOM) ? eatom : nullptr, (flags & MTP_VATOM) ? vatom : nullptr};
-  for (int k = 0; k < 8; ++k) key.p[k] = ptrs[k];
-  const bool pinned = natoms > 0 && !h->profiling && host_pinned(itypes, N * sizeof(int)) &&
-                      host_pinned(rijs, 3 * NS * sizeof(double)) && host_pinned(js, NS * sizeof(int)) &&
-                      host_pinned(jtypes, NS * sizeof(int)) && host_pinned(counts, counts ? N * sizeof(int) : 0) &&
-                      host_pinned(forces, 3 * N * sizeof(double)) &&
-                      host_pinned(key.p[6], (flags & MTP_EATOM) ? N * sizeof(double) : 0) &&
-                      host_pinned(key.p[7], (flags & MTP_VATOM) ? 6 * N * sizeof(double) : 0);
   bool launched = false;
   if (pinned && h->graph_exec && key == h->graph_key) {
     MTP_CUDA(h, cudaGraphLaunch(h->graph_exec, s));
@@ -590,8 +578,7 @@ int run_small_call(mtp_handle* h, int natoms, int stride, const int* itypes, con
     cudaGraphExec_t ex = nullptr;
     bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     if (ok) {
-      const int cst = enqueue_small_call(h, natoms, stride, itypes, rijs, js, jtypes, counts, flags, forces, eatom,
-                                         vatom);
+      const int cst = enqueue();
       const cudaError_t ce = cudaStreamEndCapture(s, &g);
       ok = cst == MTP_OK && ce == cudaSuccess && g != nullptr;
     }
@@ -613,8 +600,7 @@ int run_small_call(mtp_handle* h, int natoms, int stride, const int* itypes, con
     h->seen_uncapturable = false;
   }
   if (!launched) {
-    const int st = enqueue_small_call(h, natoms, stride, itypes, rijs, js, jtypes, counts, flags, forces, eatom,
-                                      vatom);
+    const int st = enqueue();
     if (st != MTP_OK) {
       cudaStreamSynchronize(s);   // copies from the caller's buffers complete before the error returns
       return st;
@@ -622,6 +608,30 @@ int run_small_call(mtp_handle* h, int natoms, int stride, const int* itypes, con
   }
   MTP_CUDA(h, cudaStreamSynchronize(s));
   return take_err_flags(h);
+}
+
+// One host-buffer call of mtp_compute below kPipelineMinAtoms (run_graphable).
+int run_small_call(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
+                   const int* jtypes, const int* counts, int flags, double* forces, double* eatom, double* vatom) {
+  const size_t N = natoms, NS = N * stride;
+  HostCallKey key;
+  key.kind = 0;
+  key.natoms = natoms;
+  key.stride = stride;
+  key.flags = flags & (MTP_EATOM | MTP_VATOM);
+  key.gen = h->gen;
+  const void* ptrs[8] = {itypes, rijs, js, jtypes, counts, forces,
+                         (flags & MTP_EATOM) ? eatom : nullptr, (flags & MTP_VATOM) ? vatom : nullptr};
+  for (int k = 0; k < 8; ++k) key.p[k] = ptrs[k];
+  const bool pinned = natoms > 0 && !h->profiling && host_pinned(itypes, N * sizeof(int)) &&
+                      host_pinned(rijs, 3 * NS * sizeof(double)) && host_pinned(js, NS * sizeof(int)) &&
+                      host_pinned(jtypes, NS * sizeof(int)) && host_pinned(counts, counts ? N * sizeof(int) : 0) &&
+                      host_pinned(forces, 3 * N * sizeof(double)) &&
+                      host_pinned(key.p[6], (flags & MTP_EATOM) ? N * sizeof(double) : 0) &&
+                      host_pinned(key.p[7], (flags & MTP_VATOM) ? 6 * N * sizeof(double) : 0);
+  return run_graphable(h, key, pinned, [&]() {
+    return enqueue_small_call(h, natoms, stride, itypes, rijs, js, jtypes, counts, flags, forces, eatom, vatom);
+  });
 }
 
 bool ends_with(const std::string& s, const std::string& suf) {
@@ -947,6 +957,7 @@ int mtp_compute_positions(mtp_handle* h, int nlocal, int nall, const double* x, 
     h->d_xall = nullptr;
     h->d_spall = h->d_owner = nullptr;
     h->all_cap = 0;
+    ++h->gen;
     MTP_CUDA(h, dalloc(&h->d_xall, 3 * NA));
     MTP_CUDA(h, dalloc(&h->d_spall, NA));
     MTP_CUDA(h, dalloc(&h->d_owner, NA));
@@ -957,36 +968,57 @@ int mtp_compute_positions(mtp_handle* h, int nlocal, int nall, const double* x, 
     cudaFree(h->d_neigh);
     h->d_neigh = nullptr;
     h->neigh_cap = 0;
+    ++h->gen;
     MTP_CUDA(h, dalloc(&h->d_neigh, NN));
     h->neigh_cap = NN;
   }
   if (!h->d_numneigh) MTP_CUDA(h, dalloc(&h->d_numneigh, static_cast<size_t>(h->max_atoms)));
   const int stride = h->max_nbr;
-  if (nlocal > 0) {
-    MTP_CUDA(h, cudaMemcpyAsync(h->d_xall, x, 3 * NA * sizeof(double), cudaMemcpyHostToDevice, s));
-    MTP_CUDA(h, cudaMemcpyAsync(h->d_spall, species, NA * sizeof(int), cudaMemcpyHostToDevice, s));
-    MTP_CUDA(h, cudaMemcpyAsync(h->d_owner, owner, NA * sizeof(int), cudaMemcpyHostToDevice, s));
-    MTP_CUDA(h, cudaMemcpyAsync(h->d_neigh, neigh, NN * sizeof(int), cudaMemcpyHostToDevice, s));
-    MTP_CUDA(h, cudaMemcpyAsync(h->d_numneigh, numneigh, N * sizeof(int), cudaMemcpyHostToDevice, s));
-    MTP_CUDA(h, launch_rows_from_positions(nlocal, nall, h->d_xall, h->d_spall, h->d_owner, list_stride, h->d_neigh,
-                                           h->d_numneigh, h->cutoff, stride, h->d_rijs, h->d_js, h->d_jtypes,
-                                           h->d_counts, h->d_err, s));
-  }
-  int st = run_device(h, nlocal, stride, nlocal > 0 ? h->d_spall : h->d_itypes, h->d_rijs, h->d_js, h->d_jtypes,
-                      h->d_counts, true, h->d_F, (flags & MTP_VATOM) ? h->d_vatom : nullptr);
-  if (st != MTP_OK) {
-    cudaStreamSynchronize(s);   // copies from the caller's buffers complete before the error returns
-    return st;
-  }
-  MTP_CUDA(h, launch_totals(nlocal, h->d_E, h->d_wown, h->d_partials, h->d_tot, s));
-  if (nlocal > 0) {
-    MTP_CUDA(h, cudaMemcpyAsync(forces, h->d_F, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (flags & MTP_EATOM) MTP_CUDA(h, cudaMemcpyAsync(eatom, h->d_E, N * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (flags & MTP_VATOM)
-      MTP_CUDA(h, cudaMemcpyAsync(vatom, h->d_vatom, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
-  }
-  MTP_CUDA(h, cudaMemcpyAsync(h->h_tot, h->d_tot, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
-  st = read_err_flags(h);   // synchronises the stream
+  // copies, rows, evaluation, totals and read-backs; nothing here
+  // synchronises or allocates, so run_graphable may capture it
+  auto enqueue = [&]() -> int {
+    if (nlocal > 0) {
+      MTP_CUDA(h, cudaMemcpyAsync(h->d_xall, x, 3 * NA * sizeof(double), cudaMemcpyHostToDevice, s));
+      MTP_CUDA(h, cudaMemcpyAsync(h->d_spall, species, NA * sizeof(int), cudaMemcpyHostToDevice, s));
+      MTP_CUDA(h, cudaMemcpyAsync(h->d_owner, owner, NA * sizeof(int), cudaMemcpyHostToDevice, s));
+      MTP_CUDA(h, cudaMemcpyAsync(h->d_neigh, neigh, NN * sizeof(int), cudaMemcpyHostToDevice, s));
+      MTP_CUDA(h, cudaMemcpyAsync(h->d_numneigh, numneigh, N * sizeof(int), cudaMemcpyHostToDevice, s));
+      MTP_CUDA(h, launch_rows_from_positions(nlocal, nall, h->d_xall, h->d_spall, h->d_owner, list_stride,
+                                             h->d_neigh, h->d_numneigh, h->cutoff, stride, h->d_rijs, h->d_js,
+                                             h->d_jtypes, h->d_counts, h->d_err, s));
+    }
+    int st = run_device(h, nlocal, stride, nlocal > 0 ? h->d_spall : h->d_itypes, h->d_rijs, h->d_js, h->d_jtypes,
+                        h->d_counts, true, h->d_F, (flags & MTP_VATOM) ? h->d_vatom : nullptr);
+    if (st != MTP_OK) return st;
+    MTP_CUDA(h, launch_totals(nlocal, h->d_E, h->d_wown, h->d_partials, h->d_tot, s));
+    if (nlocal > 0) {
+      MTP_CUDA(h, cudaMemcpyAsync(forces, h->d_F, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+      if (flags & MTP_EATOM)
+        MTP_CUDA(h, cudaMemcpyAsync(eatom, h->d_E, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+      if (flags & MTP_VATOM)
+        MTP_CUDA(h, cudaMemcpyAsync(vatom, h->d_vatom, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    MTP_CUDA(h, cudaMemcpyAsync(h->h_tot, h->d_tot, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    MTP_CUDA(h, cudaMemcpyAsync(h->h_err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    return MTP_OK;
+  };
+  HostCallKey key;
+  key.kind = 1;
+  key.natoms = nlocal;
+  key.stride = list_stride;
+  key.extra = nall;
+  key.flags = flags & (MTP_EATOM | MTP_VATOM);
+  key.gen = h->gen;
+  const void* ptrs[8] = {x, species, owner, neigh, numneigh, forces,
+                         (flags & MTP_EATOM) ? eatom : nullptr, (flags & MTP_VATOM) ? vatom : nullptr};
+  for (int k = 0; k < 8; ++k) key.p[k] = ptrs[k];
+  const bool pinned = nlocal > 0 && !h->profiling && host_pinned(x, 3 * NA * sizeof(double)) &&
+                      host_pinned(species, NA * sizeof(int)) && host_pinned(owner, NA * sizeof(int)) &&
+                      host_pinned(neigh, NN * sizeof(int)) && host_pinned(numneigh, N * sizeof(int)) &&
+                      host_pinned(forces, 3 * N * sizeof(double)) &&
+                      host_pinned(key.p[6], (flags & MTP_EATOM) ? N * sizeof(double) : 0) &&
+                      host_pinned(key.p[7], (flags & MTP_VATOM) ? 6 * N * sizeof(double) : 0);
+  const int st = run_graphable(h, key, pinned, enqueue);
   if (st != MTP_OK) return st;
   if (flags & MTP_EFLAG) *energy = h->h_tot[0];
   if (flags & MTP_VFLAG)

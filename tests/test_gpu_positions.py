@@ -7,13 +7,15 @@ must keep exactly the candidates a host loop keeps (pair_jax_mtp.cpp:110-167:
 so the results are bitwise those of mtp_compute on host-packed rows.
 """
 
+import ctypes
+
 import numpy as np
 import pytest
 
 from conftest import potential_path
 from mtp_b200 import synth
-from mtp_b200._lib import MTPError
-from mtp_b200.engine import MTPEngine
+from mtp_b200._lib import EATOM, EFLAG, VATOM, VFLAG, MTPError, check, lib
+from mtp_b200.engine import MTPEngine, pinned_empty
 
 pytestmark = pytest.mark.gpu
 
@@ -101,3 +103,45 @@ def test_overfull_row_is_a_capacity_error_and_the_handle_recovers():
         got = eng.compute_positions(N, x, species, owner, neigh, cut)
         assert got["energy"] == ref["energy"]
         assert np.array_equal(got["forces"], ref["forces"])
+
+
+def test_page_locked_calls_replay_a_graph_bitwise():
+    """Page-locked inputs and outputs: the second call is captured, later calls
+    replay it; every result equals the directly enqueued (pageable) call, and a
+    replay reads the positions as they are at the call."""
+    path = potential_path("cfg1md_L16_S2.mtp")
+    N, x, species, owner, lists = _system("bcc", 2.87, (3, 3, 3), 11, 2)
+    neigh, num = _pack_lists(N, lists)
+    arrays = {"x": x, "sp": species, "own": owner, "nb": neigh, "num": num}
+    pin = {}
+    for k, a in arrays.items():
+        pin[k] = pinned_empty(a.shape, a.dtype)
+        pin[k][...] = a
+    out = {"e": pinned_empty((1,)), "F": pinned_empty((N, 3)), "vir": pinned_empty((6,)),
+           "ea": pinned_empty((N,)), "va": pinned_empty((N, 6))}
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+
+    def call(eng):
+        check(lib().mtp_compute_positions(eng.handle, N, len(x), P(pin["x"]), P(pin["sp"]), P(pin["own"]),
+                                          neigh.shape[1], P(pin["nb"]), P(pin["num"]),
+                                          EFLAG | VFLAG | EATOM | VATOM, P(out["e"]), P(out["F"]), P(out["vir"]),
+                                          P(out["ea"]), P(out["va"])), eng.handle)
+        return {"energy": float(out["e"][0]), "forces": out["F"].copy(), "virial": out["vir"].copy(),
+                "site_energies": out["ea"].copy(), "vatom": out["va"].copy()}
+
+    with MTPEngine(path, N, 64, cutoff=CUTOFF) as eng:
+        eng.use_own_stream()
+        ref = eng.compute_positions(N, x, species, owner, neigh, num, eatom=True, vatom=True)
+        runs = [call(eng) for _ in range(4)]
+        st = eng.stats()
+        assert st["graph_captures"] == 1 and st["graph_replays"] == 2, st
+        for r in runs:
+            for k in ref:
+                assert np.array_equal(np.asarray(r[k]), np.asarray(ref[k])), k
+        x2 = x + np.random.default_rng(12).normal(0.0, 0.01, x.shape)
+        pin["x"][...] = x2
+        moved = call(eng)
+        assert eng.stats()["graph_replays"] == 3
+        want = eng.compute_positions(N, x2, species, owner, neigh, num, eatom=True, vatom=True)
+        for k in want:
+            assert np.array_equal(np.asarray(moved[k]), np.asarray(want[k])), k

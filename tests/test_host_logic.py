@@ -5,7 +5,9 @@
 * the C++ .mtp reader agrees with the Python one and rejects malformed files;
 * the contraction schedule (lane programs with split/combine passes), run on
   the host, reproduces the oracle's moments and dE/dm exactly in structure
-  (FP64 rounding only).
+  (FP64 rounding only);
+* the periodic ghosts and full lists handed to mtp_compute_positions, cut to
+  the cutoff, are the neighbour rows of the direct periodic builder.
 """
 
 import os
@@ -16,7 +18,7 @@ import pytest
 import torch
 
 from conftest import REPO, potential_path
-from mtp_b200 import _lib
+from mtp_b200 import _lib, synth
 from mtp_b200.engine import parse_info, schedule_emulate
 from mtp_b200.mtp_file import format_mtp, read_mtp
 from oracle import mtp_oracle as O
@@ -105,3 +107,37 @@ def test_python_writer_output_reads_back_in_cpp(tmp_path):
     f.write_text(format_mtp(p))
     info = parse_info(str(f))
     assert info["alpha_index_times_count"] == p.alpha_index_times_count
+
+
+@pytest.mark.parametrize("kind,a,reps", [("bcc", 2.87, (3, 3, 3)), ("fcc", 3.6, (4, 3, 3))])
+def test_ghosts_and_lists_give_the_periodic_rows(kind, a, reps):
+    s = synth.lattice_structure(kind, a, reps)
+    s.positions = s.positions + np.random.default_rng(4).normal(0.0, 0.08, s.positions.shape)
+    s.types = np.random.default_rng(5).integers(0, 3, s.natoms).astype(np.int32)
+    cutoff, skin = 5.0, 0.3
+    x, owner, lists = synth.ghosts_and_lists(s, cutoff + skin)
+    N = s.natoms
+    assert np.array_equal(owner[:N], np.arange(N)) and owner.min() >= 0 and owner.max() < N
+    # every ghost is a lattice translate of its owner
+    L = np.diag(s.cell)
+    shift = (x - np.mod(s.positions, L)[owner]) / L
+    assert np.allclose(shift, np.round(shift), atol=1e-12)
+    nd = synth.build_neighbors(s, cutoff)
+    for i, c in enumerate(lists):
+        d = np.linalg.norm(x[c] - x[i], axis=1)
+        assert np.all(d < cutoff + skin) and i not in c
+        inside = c[d < cutoff]
+        # the same neighbours (owner, distance) as the direct builder's row
+        got = sorted(zip(owner[inside].tolist(), np.round(d[d < cutoff], 9).tolist()))
+        row = nd.js[i, :nd.counts[i]]
+        want = sorted(zip(row.tolist(), np.round(np.linalg.norm(nd.rijs[i, :nd.counts[i]], axis=1), 9).tolist()))
+        assert got == want
+
+
+def test_ghosts_and_lists_reject_small_or_skewed_cells():
+    s = synth.lattice_structure("bcc", 2.87, (2, 2, 2))          # 5.74 A edges: not above 5.3 + a margin
+    with pytest.raises(ValueError):
+        synth.ghosts_and_lists(s, 6.0)
+    h = synth.lattice_structure("hcp", 3.0, (3, 3, 3))
+    with pytest.raises(ValueError):
+        synth.ghosts_and_lists(h, 5.0)

@@ -178,6 +178,22 @@ int mtp_compute_positions(mtp_handle* h, int nlocal, int nall, const double* x, 
                           double* vatom);
 
 /*
+ * Device-pointer variant of mtp_compute_positions: the same arguments in
+ * device memory, outputs as mtp_compute_device (energy [1], forces
+ * [nlocal][3], virial [6], optional eatom/vatom), enqueued on the handle's
+ * stream without synchronising; device-side errors (an overfull row sets
+ * MTP_E_CAPACITY) are read with mtp_sync_status.  This is the call of a
+ * pair style whose positions, species and neighbour list already live on
+ * the GPU (the reference's README.md:48 plans a Kokkos pair style; LAMMPS's
+ * KOKKOS package keeps x, type and the neighbour list in device views).
+ */
+int mtp_compute_positions_device(mtp_handle* h, int nlocal, int nall, const double* d_x,
+                                 const int* d_species, const int* d_owner, int list_stride,
+                                 const int* d_neigh, const int* d_numneigh, int flags,
+                                 double* d_energy, double* d_forces, double* d_virial,
+                                 double* d_eatom, double* d_vatom);
+
+/*
  * Device-pointer variant of mtp_compute for PyTorch and CUDA-graph capture:
  * every pointer is device memory; work is enqueued on the handle's stream and
  * the call returns without synchronising.  energy [1], virial [6].

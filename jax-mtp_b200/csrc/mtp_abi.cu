@@ -878,6 +878,41 @@ int mtp_compute_device(mtp_handle* h, int natoms, int stride, const int* d_itype
   return MTP_OK;
 }
 
+int mtp_compute_positions_device(mtp_handle* h, int nlocal, int nall, const double* d_x, const int* d_species,
+                                 const int* d_owner, int list_stride, const int* d_neigh, const int* d_numneigh,
+                                 int flags, double* d_energy, double* d_forces, double* d_virial, double* d_eatom,
+                                 double* d_vatom) {
+  if (!h) return MTP_E_INVALID;
+  if (nlocal < 0 || nall < nlocal || list_stride < 0)
+    return fail(h, MTP_E_INVALID, "need 0 <= nlocal <= nall and list_stride >= 0");
+  if (nlocal > h->max_atoms) return fail(h, MTP_E_CAPACITY, "nlocal exceeds max_atoms");
+  if (nlocal > 0 && (list_stride == 0 || !d_x || !d_species || !d_owner || !d_neigh || !d_numneigh || !d_forces))
+    return fail(h, MTP_E_INVALID, "null input or forces pointer, or list_stride 0 with atoms");
+  if ((flags & MTP_EFLAG) && !d_energy) return fail(h, MTP_E_INVALID, "MTP_EFLAG without an energy pointer");
+  if ((flags & MTP_VFLAG) && !d_virial) return fail(h, MTP_E_INVALID, "MTP_VFLAG without a virial pointer");
+  if ((flags & MTP_EATOM) && !d_eatom) return fail(h, MTP_E_INVALID, "MTP_EATOM without an eatom pointer");
+  if ((flags & MTP_VATOM) && !d_vatom) return fail(h, MTP_E_INVALID, "MTP_VATOM without a vatom pointer");
+  const int stride = h->max_nbr;
+  if (nlocal > 0)
+    MTP_CUDA(h, launch_rows_from_positions(nlocal, nall, d_x, d_species, d_owner, list_stride, d_neigh, d_numneigh,
+                                           h->cutoff, stride, h->d_rijs, h->d_js, h->d_jtypes, h->d_counts,
+                                           h->d_err, h->stream));
+  int st = run_device(h, nlocal, stride, nlocal > 0 ? d_species : h->d_itypes, h->d_rijs, h->d_js, h->d_jtypes,
+                      h->d_counts, true, d_forces, (flags & MTP_VATOM) ? d_vatom : nullptr);
+  if (st != MTP_OK) return st;
+  if (flags & (MTP_EFLAG | MTP_VFLAG)) {
+    MTP_CUDA(h, launch_totals(nlocal, h->d_E, h->d_wown, h->d_partials, h->d_tot, h->stream));
+    if (flags & MTP_EFLAG)
+      MTP_CUDA(h, cudaMemcpyAsync(d_energy, h->d_tot, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    if (flags & MTP_VFLAG)
+      MTP_CUDA(h, cudaMemcpyAsync(d_virial, h->d_tot + 1, 6 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  }
+  if ((flags & MTP_EATOM) && nlocal > 0)
+    MTP_CUDA(h, cudaMemcpyAsync(d_eatom, h->d_E, nlocal * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  h->calls++;
+  return MTP_OK;
+}
+
 int mtp_compute(mtp_handle* h, int natoms, int stride, const int* itypes, const double* rijs, const int* js,
                 const int* jtypes, const int* counts, int flags, double* energy, double* forces, double* virial,
                 double* eatom, double* vatom) {

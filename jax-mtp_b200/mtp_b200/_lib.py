@@ -39,6 +39,7 @@ SIGNATURES = {
     "mtp_compute": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "mtp_compute_device": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "mtp_compute_positions": (_I, [_P, _I, _I, _P, _P, _P, _I, _P, _P, _I, _P, _P, _P, _P, _P]),
+    "mtp_compute_positions_device": (_I, [_P, _I, _I, _P, _P, _P, _I, _P, _P, _I, _P, _P, _P, _P, _P]),
     "mtp_sync_status": (_I, [_P]),
     "mtp_compute_batch_device": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "mtp_adjoint_batch_device": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),

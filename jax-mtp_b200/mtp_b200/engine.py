@@ -252,6 +252,32 @@ class MTPEngine:
         check(code, self._h)
         return energy, forces, virial
 
+    def compute_positions_device(self, nlocal: int, x, species, owner, neigh, numneigh, *, energy=None,
+                                 forces=None, virial=None, eatom=None, vatom=None, stream=None):
+        """Device tensors in/out (mtp_compute_positions_device): x [nall, 3]
+        float64, species / owner [nall] int32, neigh [nlocal, list_stride] and
+        numneigh [nlocal] int32.  Asynchronous on ``stream`` (default: torch's
+        current stream); errors are read with ``sync_status``."""
+        import torch
+        dev = x.device
+        nall = int(species.shape[0])
+        stride = int(neigh.shape[1])
+        if forces is None:
+            forces = torch.empty((nlocal, 3), dtype=torch.float64, device=dev)
+        if energy is None:
+            energy = torch.empty(1, dtype=torch.float64, device=dev)
+        if virial is None:
+            virial = torch.empty(6, dtype=torch.float64, device=dev)
+        flags = EFLAG | VFLAG | (EATOM if eatom is not None else 0) | (VATOM if vatom is not None else 0)
+        st = torch.cuda.current_stream(dev) if stream is None else stream
+        self.set_stream(st.cuda_stream)
+        P = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
+        code = lib().mtp_compute_positions_device(self._h, nlocal, nall, P(x), P(species), P(owner), stride, P(neigh),
+                                                  P(numneigh), flags, P(energy), P(forces), P(virial), P(eatom),
+                                                  P(vatom))
+        check(code, self._h)
+        return energy, forces, virial
+
     def batch_device(self, itypes, rijs, js, jtypes, counts, cfg_of_atom, volumes, nconfig: int, stream=None):
         """Batched configurations: returns (energy [C], forces [N,3], stress [C,6] reference convention)."""
         import torch

@@ -145,3 +145,35 @@ def test_page_locked_calls_replay_a_graph_bitwise():
         want = eng.compute_positions(N, x2, species, owner, neigh, num, eatom=True, vatom=True)
         for k in want:
             assert np.array_equal(np.asarray(moved[k]), np.asarray(want[k])), k
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_pointer_variant_matches_host_variant(precision):
+    """mtp_compute_positions_device (inputs already on the GPU, as a KOKKOS-style
+    pair style holds them) gives bitwise the host-buffer variant's results, on
+    two calls in a row; an overfull row is reported by sync_status."""
+    import torch
+    path = potential_path("cfg2md_L24_S3.mtp")
+    N, x, species, owner, lists = _system("fcc", 3.6, (3, 3, 3), 13, 3)
+    neigh, num = _pack_lists(N, lists, np.random.default_rng(14))
+    dev = torch.device("cuda")
+    t = lambda a: torch.as_tensor(a).to(dev).contiguous()
+    with MTPEngine(path, N, 64, cutoff=CUTOFF, precision=precision) as eng:
+        ref = eng.compute_positions(N, x, species, owner, neigh, num, eatom=True, vatom=True)
+        for _ in range(2):
+            ea = torch.empty(N, dtype=torch.float64, device=dev)
+            va = torch.empty((N, 6), dtype=torch.float64, device=dev)
+            e, F, w = eng.compute_positions_device(N, t(x), t(species), t(owner), t(neigh), t(num), eatom=ea,
+                                                   vatom=va)
+            torch.cuda.synchronize()
+            eng.sync_status()
+            assert float(e.cpu()[0]) == ref["energy"]
+            assert np.array_equal(F.cpu().numpy(), ref["forces"])
+            assert np.array_equal(w.cpu().numpy(), ref["virial"])
+            assert np.array_equal(ea.cpu().numpy(), ref["site_energies"])
+            assert np.array_equal(va.cpu().numpy(), ref["vatom"])
+    with MTPEngine(path, N, 30, cutoff=CUTOFF, precision=precision) as eng:
+        eng.compute_positions_device(N, t(x), t(species), t(owner), t(neigh), t(num))
+        torch.cuda.synchronize()
+        with pytest.raises(MTPError, match="MTP_E_CAPACITY"):
+            eng.sync_status()

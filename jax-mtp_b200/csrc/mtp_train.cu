@@ -61,13 +61,20 @@ struct Dual2<float> {
 // a slot that it writes, so the two views do not alias (which lets the loads
 // of later entries move ahead of earlier flushes).
 template <typename T>
+struct DualOperands {
+  typename Dual2<T>::type a, b;
+};
+
+template <typename T>
 struct DualFwdBody {
+  using Operands = DualOperands<T>;
   typename Dual2<T>::type* __restrict__ V;
   const typename Dual2<T>::type* __restrict__ Vr;
   T acc, tac;
-  __device__ __forceinline__ void operator()(const uint2 e) {
+  __device__ __forceinline__ Operands load(const uint2 e) const { return {Vr[e.x & 0xFFFFu], Vr[e.x >> 16]}; }
+  __device__ __forceinline__ void apply(const uint2 e, const Operands& o) {
     const T c = entry_mult<T>(e.y);
-    const auto A = Vr[e.x & 0xFFFFu], B = Vr[e.x >> 16];
+    const auto A = o.a, B = o.b;
     acc = dev_fma(c * A.x, B.x, acc);
     tac = dev_fma(c, dev_fma(A.y, B.x, A.x * B.y), tac);
     const uint32_t op = (e.y >> kOpShift) & 3u;
@@ -89,12 +96,14 @@ struct DualFwdBody {
 //   lambda_s += c (lambda_t m_o + tau_t dm_o),  tau_s += c tau_t m_o.
 template <typename T>
 struct DualRevBody {
+  using Operands = DualOperands<T>;
   typename Dual2<T>::type* __restrict__ V;
   const typename Dual2<T>::type* __restrict__ Vr;
   T acc, tac;
-  __device__ __forceinline__ void operator()(const uint2 e) {
+  __device__ __forceinline__ Operands load(const uint2 e) const { return {Vr[e.x & 0xFFFFu], Vr[e.x >> 16]}; }
+  __device__ __forceinline__ void apply(const uint2 e, const Operands& o) {
     const T c = entry_mult<T>(e.y);
-    const auto A = Vr[e.x & 0xFFFFu], B = Vr[e.x >> 16];   // (lambda_t, tau_t), (m_o, dm_o)
+    const auto A = o.a, B = o.b;   // (lambda_t, tau_t), (m_o, dm_o)
     acc = dev_fma(c, dev_fma(A.x, B.x, A.y * B.y), acc);
     tac = dev_fma(c * A.y, B.x, tac);
     const uint32_t op = (e.y >> kOpShift) & 3u;
@@ -120,10 +129,11 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
   const int S = md.S, R = md.R, K = md.K, P = md.P, D1 = md.D + 1;
   const TrainSmem L = train_layout<T>(kVGlobal ? 0 : md.v_size, S, R, K, P, md.D, md.Sa, n_pad, NT);
   using T2 = typename Dual2<T>::type;
-  // program entries in flight per thread: with the value space in global
-  // memory two (the registers go to the dual-number operands: level 28,
-  // 32 configurations 29.2 -> 26.1 ms against four), else the evaluation's
-  constexpr int kStreamDepth = kVGlobal ? 2 : kPrefetch;
+  // program entries in flight per thread; with the value space in global
+  // memory their operand gathers are issued before any of their flushes
+  // (level 28, 32 configurations: 26.1 ms with two entries in flight and
+  // gathers at use -> 19.0 ms)
+  constexpr int kStreamDepth = kPrefetch;
   T2* V = kVGlobal ? reinterpret_cast<T2*>(vscratch) + static_cast<size_t>(blockIdx.x) * md.v_size
                    : reinterpret_cast<T2*>(smem + L.v);
   T* sRad = reinterpret_cast<T*>(smem + L.rad);
@@ -355,7 +365,7 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
     // ---- dual forward tree --------------------------------------------------
     for (int ps = 0; ps < md.nfwd; ++ps) {
       DualFwdBody<T> body{V, V, T(0), T(0)};
-      stream_entries_n<kStreamDepth>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, body);
+      stream_entries_n<kStreamDepth, kVGlobal>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, body);
       __syncthreads();
     }
     for (int a = tid; a < md.Sa; a += NT) {
@@ -367,7 +377,7 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
     // ---- dual reverse tree ---------------------------------------------------
     for (int ps = 0; ps < md.nrev; ++ps) {
       DualRevBody<T> body{V, V, T(0), T(0)};
-      stream_entries_n<kStreamDepth>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, body);
+      stream_entries_n<kStreamDepth, kVGlobal>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, body);
       __syncthreads();
     }
 

@@ -365,12 +365,18 @@ __global__ void k_partial_totals(int natoms, const double* __restrict__ e, const
   }
 }
 
+// One warp per total (7 warps): lane l adds partials l, l + 32, ... in order,
+// then a fixed butterfly over the lanes, so the order is the same on every
+// GPU and every run (a single thread walking all partials was a 256-add
+// dependent chain, 18 us of a 2,000-atom call).
 __global__ void k_final_totals(int nb, const double* __restrict__ partials, double* __restrict__ out) {
-  if (threadIdx.x < 7) {
-    double s = 0.0;
-    for (int b = 0; b < nb; ++b) s += partials[7 * b + threadIdx.x];
-    out[threadIdx.x] = s;
-  }
+  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (c >= 7) return;   // whole warps leave
+  double s = 0.0;
+  for (int b = lane; b < nb; b += 32) s += partials[7 * b + c];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[c] = s;
 }
 
 // Neighbour rows from positions, one warp per local atom: the candidates of
@@ -448,7 +454,7 @@ cudaError_t launch_totals(int natoms, const double* site_energy, const double* w
     return cudaGetLastError();
   }
   k_partial_totals<<<kReduceBlocks, 256, 0, st>>>(natoms, site_energy, wown, partials);
-  k_final_totals<<<1, 32, 0, st>>>(kReduceBlocks, partials, out);
+  k_final_totals<<<1, 7 * 32, 0, st>>>(kReduceBlocks, partials, out);
   return cudaGetLastError();
 }
 

@@ -36,8 +36,14 @@ def main(argv=None):
     ap.add_argument("--training", type=int, default=0,
                     help="instead: a batch of this many training configurations (synth.training_batch, "
                          "32-512 atoms, seed 8); one batched forward, then --calls adjoint launches")
+    ap.add_argument("--pair-call", action="store_true",
+                    help="instead: the LAMMPS-size force call, bcc a=2.87 A 10^3 cells (2,000 atoms, 50/50 "
+                         "species) with periodic ghosts and full lists (skin 0.3 A), --calls calls of "
+                         "mtp_compute_positions on page-locked buffers (max_nbr 60, cutoff 5.0 A)")
     a = ap.parse_args(argv)
     pot = read_mtp(a.potential)
+    if a.pair_call:
+        return pair_call_case(a, pot)
     if a.training:
         return training_case(a, pot)
     s = synth.config2_structure(a.reps)
@@ -93,6 +99,48 @@ def training_case(a, pot):
         eng.sync_status()
         print(json.dumps({"configs": b.nconfig, "atoms": nd.natoms, "n_pad": nd.n_pad,
                           "adjoint_ms_per_call": e0.elapsed_time(e1) / max(1, a.calls)}), flush=True)
+
+
+
+def pair_call_case(a, pot):
+    """Host wall clock of synchronous mtp_compute_positions calls (graph replay)."""
+    import ctypes
+    import time
+
+    from ._lib import EFLAG, VFLAG, check, lib
+    from .engine import pinned_empty
+    s = synth.config1()
+    s.types = s.types % pot.species_count
+    x, owner, lists = synth.ghosts_and_lists(s, 5.3)
+    N = s.natoms
+    stride = max(len(c) for c in lists)
+    buf = {"x": pinned_empty(x.shape), "sp": pinned_empty((len(x),), np.int32),
+           "own": pinned_empty((len(x),), np.int32), "nb": pinned_empty((N, stride), np.int32),
+           "num": pinned_empty((N,), np.int32), "e": pinned_empty((1,)), "F": pinned_empty((N, 3)),
+           "w": pinned_empty((6,))}
+    buf["x"][...] = x
+    buf["sp"][...] = s.types[owner]
+    buf["own"][...] = owner
+    buf["nb"][...] = -1
+    for i, c in enumerate(lists):
+        buf["nb"][i, :len(c)] = c
+        buf["num"][i] = len(c)
+    P = lambda v: v.ctypes.data_as(ctypes.c_void_p)
+    with MTPEngine(a.potential, N, 60, cutoff=5.0, precision=a.precision) as eng:
+        eng.use_own_stream()
+
+        def call():
+            check(lib().mtp_compute_positions(eng.handle, N, len(x), P(buf["x"]), P(buf["sp"]), P(buf["own"]),
+                                              stride, P(buf["nb"]), P(buf["num"]), EFLAG | VFLAG, P(buf["e"]),
+                                              P(buf["F"]), P(buf["w"]), None, None), eng.handle)
+        for _ in range(3):
+            call()
+        t0 = time.perf_counter()
+        for _ in range(a.calls):
+            call()
+        us = (time.perf_counter() - t0) / max(1, a.calls) * 1e6
+        print(json.dumps({"atoms": N, "atoms_with_ghosts": len(x), "precision": a.precision, "calls": a.calls,
+                          "us_per_call": us, "stats": eng.stats()}), flush=True)
 
 
 if __name__ == "__main__":

@@ -80,20 +80,21 @@ def algorithmic_flops(pot, counts_real: np.ndarray) -> float:
     return float(counts_real.sum()) * per_nbr + len(counts_real) * (9 * T + 2 * Sa)
 
 
-def read_traffic(threads: int, atoms_per_block: int):
-    """DRAM bytes per evaluation launch from the committed ncu summary, for the
-    launch shape that ran (lines ``traffic_bytes_per_launch_full_workload_t<T>_a<A>:``)."""
-    f = os.path.join(ROOT, "profiles", "eval_kernel_l24_mixed.md")
-    if not os.path.exists(f):
+def read_traffic(threads: int, atoms_per_block: int, precision: str = "mixed"):
+    """DRAM bytes per evaluation launch of the bench workload for the launch
+    shape that ran, from the data file that `python -m mtp_b200.profile_case
+    --write-traffic` makes out of an ncu capture (profiles/eval_kernel_traffic.json)."""
+    f = os.path.join(ROOT, "profiles", "eval_kernel_traffic.json")
+    try:
+        with open(f) as fh:
+            d = json.load(fh)
+    except (OSError, ValueError):
         return None
-    key = f"traffic_bytes_per_launch_full_workload_t{threads}_a{atoms_per_block}:"
-    for line in open(f):
-        if line.startswith(key):
-            try:
-                return float(line.split(":", 1)[1].strip())
-            except ValueError:
-                return None
-    return None
+    e = d.get(f"{precision}_t{threads}_a{atoms_per_block}")
+    if not e:
+        return None
+    return {"bytes_per_launch": float(e["bytes_per_launch_full_workload"]), "source": "eval_kernel_traffic.json",
+            "captured_atoms": e.get("captured_atoms"), "scale": e.get("scale")}
 
 
 class ClockSampler:
@@ -300,6 +301,9 @@ def run_ours(args):
                  "rms_meV_per_A": float(torch.sqrt(((fm - f64) ** 2).sum(1).mean())) * 1e3,
                  "energy_meV_per_atom": abs(em - e64) / N * 1e3,
                  "force_scale_eV_per_A": float(f64.abs().max())}
+    parity = None
+    if rank == 0 and not args.skip_cpu:
+        parity = parity_sample(pot, mds["fp64"], mds["mixed"])
     # real neighbours (d < max_dist) per atom, for the algorithmic FLOP count
     rn = mds["fp64"].rijs.norm(dim=2)
     valid = (mds["fp64"].jtypes >= 0) & (rn < pot.max_dist) & (rn > 0)
@@ -337,15 +341,14 @@ def run_ours(args):
         results[p]["eval_ms_per_launch"] = kms / max(1, kn)
         results[p]["eval_launches"] = kn
     clocks = sampler.summary()
-    # NVE drift over warm-up + timed steps (graph replays), per precision
+    # NVE drift from step 0 over `--drift-steps` steps (untimed continuation of
+    # the graph replays; one replica per process, so only without peers)
     drift = {}
+    nd_steps = args.drift_steps if world == 1 else 0
     for p in ("mixed", "fp64"):
-        nsteps = mds[p].step_count
-        e_end = mds[p].total_energy()
-        drift[p] = {"steps": nsteps, "meV_per_atom_per_ps": (e_end - e_start[p]) / N * 1e3 / (nsteps * DT)}
+        drift[p] = drift_leg(mds[p], e_start[p], max(nd_steps, mds[p].step_count))
     for p in ("mixed", "fp64"):
         mds[p].release()
-    # drift over the timed run (energy per atom)
     fp64_peak, fp32_peak = measure_fma_peak()
 
     value = job_value(N, world, args.steps, results["mixed"]["ms"])
@@ -355,7 +358,8 @@ def run_ours(args):
     achieved = flops / k_mixed / 1e12
     achieved64 = flops / k_64 / 1e12
     ran = tuning["mixed"]["ran"]
-    traffic = read_traffic(ran["threads"], ran["atoms_per_block"])
+    traffic_rec = read_traffic(ran["threads"], ran["atoms_per_block"])
+    traffic = traffic_rec["bytes_per_launch"] if traffic_rec else None
     # the same launch against HBM: algorithmic bytes per atom-step through the
     # evaluation (28 n_pad + 36: r_ij and neighbour index in, force and energy out)
     alg_bytes = (28 * STRIDE + 36) * N
@@ -384,6 +388,10 @@ def run_ours(args):
     if rank == 0 and not args.skip_cpu:
         cpu = cpu_baseline(pot, s, seconds=args.cpu_seconds)
 
+    pair_nve = None
+    if rank == 0 and world == 1 and not args.skip_e2e and args.pair_nve_steps > 0:
+        pair_nve = run_pair_style_nve(args.pair_nve_steps)
+
     for p in ("mixed", "fp64"):
         eng[p].close()
     del mds
@@ -402,10 +410,12 @@ def run_ours(args):
             "mixed_over_fp64": value / value64,
             "force_error_mixed_vs_fp64": force_err,
             "nve_drift": drift,
+            "parity_sample": parity,
             "autotuned_launch": tuning,
             "train": train,
             "roofline": {"bound": "fp32-fma", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
+                         "traffic_record": traffic_rec,
                          "kernel": "k_mtp_eval<float> (mixed)", "flops_per_launch": flops,
                          "kernel_ms": k_mixed * 1e3, "hbm_view": hbm_view,
                          "peak_source": "measured live: FP32 FMA-chain kernel (no FP32/FP64 CUDA-core peak in "
@@ -415,6 +425,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "pair_style_call": pair_call,
+            "pair_style_nve_config1": pair_nve,
             "gpu_launches": launches * 1,
             "clocks": clocks,
         }
@@ -423,6 +434,148 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def parity_sample(pot, md64, mdmx, nsample: int = 512, seed: int = 54):
+    """Oracle spot-check of the bench's own rows: `nsample` random atoms of the
+    1,048,576-atom system at the starting configuration, their site energies
+    and forces from the FP64 and mixed kernels against the C++ FP64 oracle
+    (oracle/mtp_cpu.cpp).  The oracle evaluates the sampled atoms and every
+    neighbour of theirs (the full lists are symmetric, so every slot that points
+    at a sampled atom belongs to that set), which makes the sampled forces
+    exact."""
+    import torch
+    from oracle.cpu_ref import CpuMTP
+    N = md64.N
+    out = {}
+    gpu = {}
+    for tag, md in (("fp64", md64), ("mixed", mdmx)):
+        eat = torch.empty(N, dtype=torch.float64, device=md.x.device)
+        E, F, W = md.eng.compute_device(md.types, md.rijs, md.js, md.jtypes, md.counts, eatom=eat)
+        torch.cuda.synchronize()
+        gpu[tag] = (eat.cpu().numpy(), F.cpu().numpy())
+    rng = np.random.default_rng(seed)
+    pick = np.sort(rng.choice(N, nsample, replace=False))
+    js = md64.js.cpu().numpy()
+    jt = md64.jtypes.cpu().numpy()
+    cnt = md64.counts.cpu().numpy()
+    rows = js[pick]
+    nb = rows[(jt[pick] >= 0) & (np.arange(js.shape[1])[None, :] < cnt[pick][:, None]) & (rows >= 0)]
+    closure = np.unique(np.concatenate([pick, nb]))
+    remap = np.full(N, -1, dtype=np.int64)
+    remap[closure] = np.arange(len(closure))
+    sub_js = js[closure]
+    sub_js = np.where(sub_js >= 0, remap[np.clip(sub_js, 0, N - 1)], -1).astype(np.int32)
+    rij = md64.rijs.cpu().numpy()[closure]
+    ref = CpuMTP(pot).compute(md64.types.cpu().numpy()[closure], rij, sub_js, jt[closure], cnt[closure],
+                              nthreads=os.cpu_count() or 1)
+    at = remap[pick]
+    e_ref, f_ref = ref["site_energies"][at], ref["forces"][at]
+    for tag in ("fp64", "mixed"):
+        e, f = gpu[tag][0][pick], gpu[tag][1][pick]
+        out[tag] = {"site_energy_max_rel": float(np.abs(e - e_ref).max() / np.abs(e_ref).max()),
+                    "force_max_rel": float(np.abs(f - f_ref).max() / np.abs(f_ref).max()),
+                    "site_energy_max_abs_meV": float(np.abs(e - e_ref).max() * 1e3),
+                    "force_max_abs_meV_per_A": float(np.abs(f - f_ref).max() * 1e3)}
+    out["atoms_sampled"] = int(nsample)
+    out["oracle_atoms_evaluated"] = int(len(closure))
+    out["reference"] = "C++ FP64 restatement (oracle/mtp_cpu.cpp), same rows"
+    out["bars"] = {"fp64_rel": 1e-10, "mixed_site_energy_meV": 0.1, "mixed_force_meV_per_A": 1.0}
+    return out
+
+
+def drift_leg(md, e0: float, nsteps: int, every: int = 10):
+    """NVE total-energy record from step 0 (`e0`) to `nsteps` MD steps,
+    continuing the graph replays of the timed run (untimed).  The drift is
+    the least-squares slope of E_total(t); the end-point difference and the
+    largest excursion are reported beside it."""
+    ts, es = [0], [e0]
+    if md.step_count > 0:
+        ts.append(md.step_count)
+        es.append(md.total_energy())
+    while md.step_count < nsteps:
+        md.run(min(every, nsteps - md.step_count), graphs=True)
+        ts.append(md.step_count)
+        es.append(md.total_energy())
+    t = np.asarray(ts, dtype=np.float64) * DT
+    e = np.asarray(es, dtype=np.float64)
+    slope = float(np.polyfit(t, e, 1)[0]) if len(t) > 1 else 0.0
+    N = md.N
+    return {"steps": int(md.step_count), "samples": len(ts),
+            "meV_per_atom_per_ps": slope / N * 1e3,
+            "endpoint_meV_per_atom_per_ps": (e[-1] - e[0]) / N * 1e3 / max(t[-1], 1e-30),
+            "max_excursion_meV_per_atom": float(np.abs(e - e[0]).max() / N * 1e3),
+            "method": "least-squares slope of total energy over the run"}
+
+
+def run_pair_style_nve(steps: int = 1000):
+    """Config 1 through the pair style: `pair_style jax/mtp` driven by the mini
+    LAMMPS host driver (host neighbour list with ghosts, rebuild every 10 steps,
+    skin 0.3 A, rows built on the GPU from positions), level-16 MD potential,
+    2 species, bcc a = 2.87 A, 10^3 cells = 2,000 atoms, MAX_ATOMS_PER_NEIGHBOR
+    60, Maxwell-Boltzmann 300 K (seed 4), dt 1 fs.  atom-steps/s is the
+    driver's host wall clock over the whole MD loop (integration, lists,
+    pair-style calls)."""
+    import tempfile
+    from mtp_b200 import synth
+    from mtp_b200.lammps_data import write_data
+    pdir = os.path.join(ROOT, "jax-mtp_b200", "pair_style")
+    r = subprocess.run(["make", "-C", pdir], capture_output=True, text=True)
+    if r.returncode != 0:
+        return {"unavailable": "mini LAMMPS driver did not build: " + r.stderr[-300:]}
+    s = synth.config1()
+    v = synth.maxwell_boltzmann(s.natoms, 300.0, MASS, seed=4)
+    pot = os.path.join(ROOT, "tests", "golden", "potentials", "cfg1md_L16_S2.mtp")
+    out = {"workload": "pair_style jax/mtp NVE, level-16 MD potential, 2 species, bcc a=2.87 A 10^3 = 2,000 atoms, "
+                       "300 K, dt 1 fs, rebuild every 10 steps (skin 0.3 A), 60 slots per row",
+           "steps": steps, "timer": "host wall clock of the driver's MD loop"}
+    with tempfile.TemporaryDirectory() as td:
+        data = os.path.join(td, "data.txt")
+        write_data(data, s, v, 2)
+        for prec in ("fp64", "mixed"):
+            r = subprocess.run([os.path.join(pdir, "_build", "mini_lammps"), data, pot, str(s.natoms), "60", "5.0",
+                                str(MASS), str(DT), str(steps), "10", "0.3", prec, "100"],
+                               capture_output=True, text=True, timeout=900)
+            if r.returncode != 0:
+                out[prec] = {"error": r.stderr[-300:]}
+                continue
+            lines = r.stdout.strip().splitlines()
+            summ = json.loads(lines[-1])
+            th = [l.split() for l in lines if l.startswith("step")]
+            t = np.array([float(x[1]) for x in th]) * DT
+            et = np.array([float(x[7]) for x in th])
+            slope = float(np.polyfit(t, et, 1)[0]) if len(t) > 1 else 0.0
+            out[prec] = {"atom_steps_per_s": summ["atom_steps_per_s"], "pair_ms_per_step": summ["pair_ms_per_step"],
+                         "drift_meV_per_atom_per_ps": slope / s.natoms * 1e3,
+                         "endpoint_drift_meV_per_atom": summ["energy_drift_eV_per_atom"] * 1e3,
+                         "temperature_end_K": float(th[-1][9]), "pair_calls": summ["pair_calls"]}
+    return out
+
+
+def batch_diagnostics(nds, min_dist: float):
+    """How much of a training batch lies below the potential's min_dist, where
+    the Chebyshev basis is evaluated outside [-1, 1] (the stated lattice range
+    a in [2.8, 4.2] A puts fcc nearest neighbours at 1.98-2.97 A)."""
+    n_pairs = n_bad = n_cfg_bad = 0
+    dmin = float("inf")
+    for nd in nds:
+        d = np.linalg.norm(nd.rijs, axis=2)[nd.jtypes >= 0]
+        b = int((d < min_dist).sum())
+        n_pairs += d.size
+        n_bad += b
+        n_cfg_bad += b > 0
+        if d.size:
+            dmin = min(dmin, float(d.min()))
+    return {"pairs_below_min_dist_frac": n_bad / max(1, n_pairs), "configs_with_pairs_below_min_dist": n_cfg_bad,
+            "configs": len(nds), "min_pair_distance_A": dmin, "min_dist_A": min_dist}
+
+
+def rmse_per_atom(E, F, E_t, F_t, natom_c):
+    """Energy RMSE per atom (meV/atom) over configurations and force RMSE (meV/A) over components."""
+    import torch
+    de = ((E - E_t) / natom_c)
+    return {"energy_rmse_meV_per_atom": float(torch.sqrt((de * de).mean())) * 1e3,
+            "force_rmse_meV_per_A": float(torch.sqrt(((F - F_t) ** 2).mean())) * 1e3}
 
 
 def run_train(args, device, dist):
@@ -463,8 +616,11 @@ def run_train(args, device, dist):
     with MTPEngine(os.path.join(potdir, "cfg3label_L20_S2.mtp"), nd.natoms, nd.n_pad) as lab:
         E_l, F_l, S_l = lab.batch_device(batch.itypes, batch.rijs, batch.js, batch.jtypes, batch.counts, batch.cfg,
                                          batch.volumes, batch.nconfig)
+    diag3 = batch_diagnostics(nds, pot3.min_dist)
     g = torch.Generator(device="cpu").manual_seed(7)
     natom_c = torch.as_tensor(np.diff(offs), dtype=torch.float64, device=device)
+    diag3["label_energy_rms_eV_per_atom"] = float(torch.sqrt(((E_l / natom_c) ** 2).mean()))
+    diag3["label_force_rms_eV_per_A"] = float(torch.sqrt((F_l ** 2).mean()))
     E_t = E_l + 1e-3 * natom_c * torch.randn(batch.nconfig, generator=g, dtype=torch.float64).to(device)
     F_t = F_l + 1e-2 * torch.randn(F_l.shape, generator=g, dtype=torch.float64).to(device)
     S_t = S_l + 6.2415e-4 * torch.randn(S_l.shape, generator=g, dtype=torch.float64).to(device)
@@ -477,6 +633,7 @@ def run_train(args, device, dist):
         E_p, F_p, S_p = eng3.batch_device(batch.itypes, batch.rijs, batch.js, batch.jtypes, batch.counts, batch.cfg,
                                           batch.volumes, batch.nconfig)
         loss = float(weighted_loss(E_p, F_p, S_p, (E_t, F_t, S_t)))
+        rmse3 = rmse_per_atom(E_p, F_p, E_t, F_t, natom_c)
         eng3.sync_status()
     # least-squares basis fit of configuration 3 (FP64): Jacobian by 289
     # batched forwards, then a thin SVD (the reference's jacfwd + lstsq)
@@ -487,20 +644,31 @@ def run_train(args, device, dist):
         theta, info = solve_lls_basis(e64, batch, (E_t, F_t, S_t), pot3.species_coeffs, pot3.radial_coeffs)
         torch.cuda.synchronize(device)
         lls_s = time.perf_counter() - t0
+        with torch.no_grad():
+            E_f, F_f, _ = predict({"species": torch.as_tensor(pot3.species_coeffs, device=device),
+                                   "basis": theta, "radial": torch.as_tensor(pot3.radial_coeffs, device=device)},
+                                  e64, batch)
+        rmse_fit = rmse_per_atom(E_f, F_f, E_t, F_t, natom_c)
         e64.sync_status()
     out["cfg3_lls_basis"] = {"seconds": lls_s, "forwards": pot3.alpha_scalar_moments + 1, "rank": info["rank"],
                              "loss_after": info["loss"], "loss_before": loss, "precision": "fp64",
+                             "rmse_before": rmse3, "rmse_after": rmse_fit,
                              "rows": int(batch.nconfig * 7 + 3 * batch.natoms)}
     out["cfg3_batched_forward"] = {"value": world * batch.nconfig * steps / (ms * 1e-3), "unit": "cfg/s",
                                    "configs": batch.nconfig, "atoms": batch.natoms, "nbr_stride": nd.n_pad,
                                    "ms_per_batch": ms / steps, "precision": "mixed", "loss_vs_labels": loss,
+                                   "rmse_vs_labels": rmse3, "data_diagnostics": diag3,
                                    "labels": "second random level-20 MTP (seed 7) + noise 1 meV/atom, "
-                                             "10 meV/A, 0.1 GPa"}
+                                             "10 meV/A, 0.1 GPa",
+                                   "note": "the raw loss is dominated by the configurations with pairs below "
+                                           "min_dist, where both random potentials extrapolate the Chebyshev "
+                                           "basis; the throughput is unaffected"}
     del batch
     # ---- configuration 4: forward + adjoint training step, FP64
     pot4 = read_mtp(os.path.join(potdir, "cfg4_L28_S4.mtp"))
     structs = synth.training_batch(256, 32, 512, 4, seed=8)
     nds = [synth.build_neighbors(st, pot4.max_dist) for st in structs]
+    diag4 = batch_diagnostics(nds, pot4.min_dist)
     nd, cfg, offs, vols = synth.pack_batch(nds)
     batch = DeviceBatch.from_numpy(nd, cfg, vols, device=device)
     with MTPEngine(os.path.join(potdir, "cfg4_L28_S4.mtp"), nd.natoms, nd.n_pad, precision="fp64") as eng4:
@@ -527,7 +695,8 @@ def run_train(args, device, dist):
                               "configs": batch.nconfig, "atoms": batch.natoms, "nbr_stride": nd.n_pad,
                               "ms_per_step": ms / steps, "precision": "fp64",
                               "step": "batched forward (E, F, stress) + loss + hand-written adjoint w.r.t. all "
-                                      "coefficients", "jax_grad_baseline": "unavailable on this box (no JAX)"}
+                                      "coefficients", "jax_grad_baseline": "unavailable on this box (no JAX)",
+                              "data_diagnostics": diag4}
     return out
 
 
@@ -564,7 +733,7 @@ def run_e2e(eng, md, N, args):
 
     for _ in range(max(1, min(args.warmup, 2))):
         call()
-    steps = max(1, min(args.steps, 5))
+    steps = max(5, min(args.steps, 20))
     t0 = time.perf_counter()
     for _ in range(steps):
         call()
@@ -678,6 +847,10 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--skip-train", action="store_true")
+    ap.add_argument("--drift-steps", type=int, default=500,
+                    help="NVE drift record length in MD steps (untimed; 1 GPU only; 0: the timed steps only)")
+    ap.add_argument("--pair-nve-steps", type=int, default=1000,
+                    help="config 1 through the pair style: MD steps of the mini LAMMPS driver (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

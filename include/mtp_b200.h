@@ -313,7 +313,10 @@ int mtp_profile_read(mtp_handle* h, double* eval_ms, int* eval_launches);
  * (natoms * nbr_stride); larger inputs, or a basis whose value space does
  * not fit in shared memory, return MTP_E_CAPACITY.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress), so make
- * that first call before any stream capture.  All calls share the array:
+ * that first call before any stream capture.  The address is kept for the
+ * life of the process: after cudaDeviceReset (or anything else that destroys
+ * the device's primary context) it is stale, so do not use this entry point
+ * again in that process.  All calls share the array:
  * calls that overlap on the GPU (several streams, several handles) race.
  */
 #define MTP_NOALLOC_MAX_ATOMS 16384

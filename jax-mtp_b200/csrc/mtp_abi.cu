@@ -181,6 +181,7 @@ DevModel make_model(mtp_handle* h, const DeviceSchedule& ds) {
   md.dense_k = h->d_dense_k;
   md.Q = s.Q;
   md.npairs = s.npairs;
+  md.tri = s.tri ? 1 : 0;
   for (int v = 0; v <= s.D; ++v) md.nmu[v] = s.nmu[v];
   md.S = h->pot.S;
   md.R = h->pot.R;
@@ -1385,7 +1386,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAlloc.total]
 
 // Device address of g_noalloc_scratch on the current device.  In host code
 // the symbol is only a host-side stand-in, so the address is asked for once
-// per device (with that device current) and cached.
+// per device (with that device current) and cached for the life of the
+// process; a reset of the device's primary context (cudaDeviceReset) makes the
+// cached address stale, which the header states as a limit of this path.
 int noalloc_base(mtp_handle* h, unsigned char** out) {
   static std::mutex mu;
   static unsigned char* base[64] = {};
@@ -1427,16 +1430,22 @@ int mtp_compute_device_noalloc(mtp_handle* h, int natoms, int stride, const int*
   if (st != MTP_OK) return st;
   const bool fp64 = h->precision == MTP_PRECISION_FP64;
 
-  // launch shape from the schedules already on the device; the value space
+  // launch shape from the schedules already on the device, each paired only
+  // with the atoms per block whose operand width its entry order was tuned
+  // for, within the handle's launch limits (mtp_set_launch); the value space
   // must fit in shared memory (its global-memory form would need an allocation)
   const DeviceSchedule* ds = nullptr;
   int lanes = 0, A = 1, bps = 0, best = -1;
   for (const auto& kv : h->scheds) {
     const DevModel md = make_model(h, kv.second);
     const int sl = kv.second.sched.lanes;
+    if (sl > h->threads) continue;
     for (int a : {4, 2, 1}) {
       if (!eval_variant_exists(fp64, false, a)) continue;
-      const int b = eval_blocks_per_sm(md, stride, sl, fp64, false, a);
+      if (h->apb > 0 && a != h->apb) continue;
+      if (kv.second.sched.width != access_width(fp64, a)) continue;
+      int b = eval_blocks_per_sm(md, stride, sl, fp64, false, a);
+      if (h->blocks_per_sm > 0) b = std::min(b, h->blocks_per_sm);
       if (b <= 0) continue;
       const int score = (a * b) * 1024 + b * sl / 32;
       if (score > best) {
@@ -1450,8 +1459,9 @@ int mtp_compute_device_noalloc(mtp_handle* h, int natoms, int stride, const int*
   }
   if (!ds)
     return fail(h, MTP_E_CAPACITY,
-                "the value space of this basis does not fit in shared memory; the allocation-free path cannot "
-                "place it in global memory");
+                "no uploaded schedule gives a shared-memory launch within the handle's launch limits (either the "
+                "value space of this basis does not fit in shared memory, which the allocation-free path cannot "
+                "replace by global memory, or no allocating call has uploaded a schedule for these limits yet)");
 
   double* grad = reinterpret_cast<double*>(base + kNoAlloc.grad);
   double* energy = reinterpret_cast<double*>(base + kNoAlloc.energy);

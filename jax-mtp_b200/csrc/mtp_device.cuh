@@ -64,6 +64,7 @@ struct DevModel {
   int nseed, nzero;
   int S, R, K, M, B, P, D, Sa;
   int Q, npairs;
+  int tri;                  // Schedule::tri: step k of a force-phase chain has k / 2 + 1 radial functions
   int nmu[kMaxDegree + 1];  // radial functions with a basic moment of each degree
   int v_m, v_dm, v_zero, v_one, v_size;
   double scaling, rmin, rmax;
@@ -279,7 +280,12 @@ __device__ __forceinline__ void stream_entries_n(const uint2* __restrict__ ent, 
 // side by side.  The tpn threads of a neighbour pair take the (a, b)
 // pairs in snake order (sl, 2 tpn-1-sl, 2 tpn+sl, ...) of the pair order
 // (a + b ascending), so their shares differ by one pair at most.
-template <typename T, int R, bool kTwo>
+// kTri (Schedule::tri): the chain's step k = top - c has table entries for
+// mu <= k / 2 only (the others are zero); the chain is unrolled over k so each
+// step does exactly those multiply-adds (level 24: 581 of the dense table's
+// 1,716 (slot, mu) entries).  The sums keep the dense order with the zero
+// terms left out.
+template <typename T, int R, bool kTwo, bool kTri>
 __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
                                         int npairs, int D1, const T* __restrict__ fq0, const T* __restrict__ fpq0,
                                         const T* __restrict__ fq1, const T* __restrict__ fpq1, bool two,
@@ -308,17 +314,19 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
     const int ea = i - sb, eb = s - ea, top = D - s;
     const T* drow = dmt + (slot_sb + ea * (D - s + 1) + top) * R;
     T h0 = T(0), hz0 = T(0), hs0 = T(0), h1 = T(0), hz1 = T(0), hs1 = T(0);
-#pragma unroll 1
-    for (int c = top; c >= 0; --c, drow -= R) {
+    // one Horner step: table row drow, radial functions mu < nm
+    auto step = [&](const T* row, int nm) {
       T w0 = T(0), wp0 = T(0), w1 = T(0), wp1 = T(0);
 #pragma unroll
       for (int mu = 0; mu < R; ++mu) {
-        const T g = drow[mu];
-        w0 = dev_fma(g, f0[mu], w0);
-        wp0 = dev_fma(g, fp0[mu], wp0);
-        if (kTwo) {
-          w1 = dev_fma(g, f1[mu], w1);
-          wp1 = dev_fma(g, fp1[mu], wp1);
+        if (mu < nm) {
+          const T g = row[mu];
+          w0 = dev_fma(g, f0[mu], w0);
+          wp0 = dev_fma(g, fp0[mu], wp0);
+          if (kTwo) {
+            w1 = dev_fma(g, f1[mu], w1);
+            wp1 = dev_fma(g, fp1[mu], wp1);
+          }
         }
       }
       hz0 = dev_fma(hz0, uz0, h0);
@@ -329,6 +337,16 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
         h1 = dev_fma(h1, uz1, w1);
         hs1 = dev_fma(hs1, uz1, wp1);
       }
+    };
+    if (kTri) {
+#pragma unroll
+      for (int k = 0; k <= kMaxDegree; ++k) {
+        if (k > top) break;
+        step(drow - k * R, k / 2 + 1);
+      }
+    } else {
+#pragma unroll 1
+      for (int c = top; c >= 0; --c, drow -= R) step(drow, R);
     }
     {
       const T xa = pw0[ea], yb = pw0[D1 + eb];
@@ -715,8 +733,14 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
           switch (R) {
 #define MTP_N3_CASE(RR)                                                                                        \
   case RR:                                                                                                     \
-    n3_sums<T, RR, kTwoN>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R, sFp + qb * R, \
-                   two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2], sU[4 * qb + 2], sl, tpn, Ssum, Gx, Gy, Gz); \
+    if (md.tri)                                                                                                \
+      n3_sums<T, RR, kTwoN, true>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R,          \
+                                  sFp + qb * R, two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2],          \
+                                  sU[4 * qb + 2], sl, tpn, Ssum, Gx, Gy, Gz);                                 \
+    else                                                                                                       \
+      n3_sums<T, RR, kTwoN, false>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R,         \
+                                   sFp + qb * R, two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2],         \
+                                   sU[4 * qb + 2], sl, tpn, Ssum, Gx, Gy, Gz);                                \
     break;
             MTP_N3_CASE(1) MTP_N3_CASE(2) MTP_N3_CASE(3) MTP_N3_CASE(4)
             MTP_N3_CASE(5) MTP_N3_CASE(6) MTP_N3_CASE(7) MTP_N3_CASE(8)

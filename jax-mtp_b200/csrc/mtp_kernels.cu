@@ -247,12 +247,16 @@ cudaError_t launch_incoming(int natoms, int stride, const int* js, const int* jt
                             int* in_cnt, int* in_ptr, int* in_cursor, int* in_slot, int* block_tmp,
                             cudaStream_t st) {
   if (natoms <= 0) return cudaSuccess;
-  cudaMemsetAsync(in_cnt, 0, sizeof(int) * natoms, st);
-  cudaMemsetAsync(in_cursor, 0, sizeof(int) * natoms, st);
+  // both counters must start at zero (the allocation-free path reuses a
+  // shared array that still holds the previous call's values)
+  cudaError_t e = cudaMemsetAsync(in_cnt, 0, sizeof(int) * natoms, st);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(in_cursor, 0, sizeof(int) * natoms, st);
+  if (e != cudaSuccess) return e;
   const size_t n = static_cast<size_t>(natoms) * stride;
   const int gb = static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 32));
   k_count_incoming<<<gb, 256, 0, st>>>(natoms, stride, js, jtypes, counts, in_cnt);
-  cudaError_t e = scan_exclusive(natoms, in_cnt, in_ptr, block_tmp, st);
+  e = scan_exclusive(natoms, in_cnt, in_ptr, block_tmp, st);
   if (e != cudaSuccess) return e;
   k_fill_incoming<<<gb, 256, 0, st>>>(natoms, stride, js, jtypes, counts, in_ptr, in_cursor, in_slot);
   k_sort_incoming<<<static_cast<unsigned>((static_cast<size_t>(natoms) * 32 + 255) / 256), 256, 0, st>>>(

@@ -513,6 +513,11 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
       }
     }
   }
+  s.tri = true;
+  for (int k = 0; k < B; ++k) {
+    const int deg = pot.basic[4 * k + 1] + pot.basic[4 * k + 2] + pot.basic[4 * k + 3];
+    if (2 * pot.basic[4 * k] > s.D - deg) s.tri = false;
+  }
   // moments that are read but never written stay zero for the whole run
   std::vector<char> read(M, 0);
   for (int e = 0; e < T; ++e) { read[pot.times[4 * e]] = 1; read[pot.times[4 * e + 1]] = 1; }

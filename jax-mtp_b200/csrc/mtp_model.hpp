@@ -88,6 +88,11 @@ struct Schedule {
   int Q = 0;                    // (D+1)(D+2)(D+3)/6 slots
   int npairs = 0;               // (D+1)(D+2)/2 pairs
   std::vector<int> dense_k;     // [Q][kMaxR] basic-moment index of slot and mu, or -1
+  // Every basic moment (mu, a, b, c) has 2 mu <= D - (a + b + c): the radial
+  // function mu only meets monomials of degree <= D - 2 mu (true of every
+  // level-defined MTP basis).  Then a force-phase Horner step k = D - degree
+  // has nonzero table entries for mu <= k / 2 only.
+  bool tri = false;
   std::vector<int> zero_list;   // non-basic moments never written (must read as 0)
   std::vector<Pass> fwd, rev;   // passes in execution order
   std::vector<uint32_t> entries;  // pairs (x, y) per entry: 2 words; kStepAlign no-op rows at the end

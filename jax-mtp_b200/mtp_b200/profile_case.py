@@ -1,4 +1,6 @@
-"""A bounded evaluation case for profilers (ncu) and quick timing.
+"""Profiling harness (not part of the library's API): a bounded evaluation case
+for profilers (ncu) and quick timing, the command every ncu summary of the
+evaluation and adjoint kernels was captured with.
 
     python -m mtp_b200.profile_case --potential <file.mtp> --reps 32 --precision mixed --calls 3
 
@@ -23,9 +25,55 @@ from .engine import MTPEngine
 from .mtp_file import read_mtp
 
 
+_BYTE_UNITS = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "Tbyte": 1e12,
+               "KB": 1e3, "MB": 1e6, "GB": 1e9}
+
+
+def write_traffic(json_path: str, csv_path: str, key: str, kernel: str, scale: float, captured_atoms: int) -> dict:
+    """DRAM bytes per launch of `kernel` from `ncu -i <rep> --page raw --csv`
+    output (dram__bytes_read.sum + dram__bytes_write.sum, averaged over the
+    captured launches), scaled by `scale` to the full workload, merged into
+    the JSON data file under `key`."""
+    import csv
+    rows = list(csv.reader(open(csv_path)))
+    head = rows[0]
+    units = rows[1]
+    iname = head.index("Kernel Name")
+    irx, iwx = head.index("dram__bytes_read.sum"), head.index("dram__bytes_write.sum")
+    per = []
+    for r in rows[2:]:
+        if len(r) <= max(irx, iwx) or kernel not in r[iname]:
+            continue
+        rb = float(r[irx].replace(",", "")) * _BYTE_UNITS[units[irx]]
+        wb = float(r[iwx].replace(",", "")) * _BYTE_UNITS[units[iwx]]
+        per.append(rb + wb)
+    if not per:
+        raise SystemExit(f"no launch of {kernel!r} in {csv_path}")
+    entry = {"bytes_per_launch_captured": sum(per) / len(per), "launches": len(per), "scale": scale,
+             "captured_atoms": captured_atoms, "bytes_per_launch_full_workload": scale * sum(per) / len(per),
+             "kernel": kernel}
+    try:
+        with open(json_path) as fh:
+            data = json.load(fh)
+    except (OSError, ValueError):
+        data = {}
+    data[key] = entry
+    with open(json_path, "w") as fh:
+        json.dump(data, fh, indent=1, sort_keys=True)
+        fh.write("\n")
+    return entry
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--potential", required=True)
+    ap.add_argument("--write-traffic", metavar="JSON",
+                    help="instead: merge the DRAM bytes per launch of --ncu-csv (ncu --page raw --csv) into JSON "
+                         "under --key, scaled by --scale to the full workload")
+    ap.add_argument("--ncu-csv")
+    ap.add_argument("--key")
+    ap.add_argument("--kernel", default="k_mtp_eval")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--potential")
     ap.add_argument("--reps", type=int, default=32)
     ap.add_argument("--stride", type=int, default=64)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
@@ -41,6 +89,12 @@ def main(argv=None):
                          "species) with periodic ghosts and full lists (skin 0.3 A), --calls calls of "
                          "mtp_compute_positions on page-locked buffers (max_nbr 60, cutoff 5.0 A)")
     a = ap.parse_args(argv)
+    if a.write_traffic:
+        e = write_traffic(a.write_traffic, a.ncu_csv, a.key, a.kernel, a.scale, 4 * a.reps ** 3)
+        print(json.dumps(e))
+        return 0
+    if not a.potential:
+        ap.error("--potential is required")
     pot = read_mtp(a.potential)
     if a.pair_call:
         return pair_call_case(a, pot)

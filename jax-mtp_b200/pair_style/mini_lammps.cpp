@@ -11,8 +11,20 @@
 //
 // usage: mini_lammps <data.txt> <potential.mtp> <max_atoms> <max_nbr> <cutoff> <mass_amu>
 //                    <dt_ps> <steps> <every> <skin> [fp64|mixed] [thermo_every]
+//                    [device|host rows] [nve|boxrelax] [ftol_eV_per_A] [ptol_bar] [out.txt]
 // data.txt: "natoms ntypes" / "Lx Ly Lz" / natoms lines "tag type x y z vx vy vz"
 // (orthorhombic box [0, L)).  Prints thermo lines and a final JSON summary.
+//
+// Mode nve (default): velocity Verlet for <steps> steps (LAMMPS `fix nve`).
+// Mode boxrelax: the energy minimisation of the reference's own input,
+// `fix box/relax iso 0.0` + `minimize` (test_lammps.in:27-28), driven by the
+// pair style's virial: atoms relax by FIRE at fixed box until max |F| <
+// ftol, then the box is rescaled isotropically (atoms affinely) by a secant
+// step on the pressure P = (W_xx + W_yy + W_zz) / (3 V) towards zero, for at
+// most <steps> box updates or until |P| < ptol with the atoms relaxed.
+// Prints one "relax" line per box update and a final JSON summary with the
+// box, the energy and the pressure; with out.txt, the final box and local
+// atoms are written there in the data-file format (zero velocities).
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -150,12 +162,116 @@ void build_list(Sim& s, double rcut) {
   for (int i = 0; i < s.nlocal; ++i) s.firstneigh[i] = s.pages.data() + start[i];
 }
 
+constexpr double kNktv2p = 1.6021765e6;   // eV/A^3 -> bar (LAMMPS metal)
+
+// Total force on the local atoms after the ghost forces went to their owners.
+double max_force(const Sim& s) {
+  double m = 0.0;
+  for (int i = 0; i < s.nlocal; ++i)
+    for (int a = 0; a < 3; ++a) m = std::max(m, std::fabs(s.fbuf[3 * i + a]));
+  return m;
+}
+
+void fold_ghost_forces(Sim& s) {
+  for (int g = 0; g < s.nghost; ++g)
+    for (int a = 0; a < 3; ++a) s.fbuf[3 * s.ghost_owner[g] + a] += s.fbuf[3 * (s.nlocal + g) + a];
+}
+
+// fix box/relax iso 0.0 + minimize, as alternating FIRE atom relaxation at
+// fixed box and secant steps of the isotropic box length on the pressure.
+template <typename Pair, typename Rebuild, typename Bind, typename Force>
+int box_relax(Sim& s, Pair& pair, Rebuild rebuild, Bind bind, Force force_call, double mass, double dt,
+              int max_box_steps, double ftol, double ptol_bar) {
+  auto evaluate = [&](double* pe, double* press) {
+    rebuild();
+    bind();
+    force_call(1, 1);
+    fold_ghost_forces(s);
+    const double vol = s.L[0] * s.L[1] * s.L[2];
+    *pe = pair.eng_vdwl;
+    *press = (pair.virial[0] + pair.virial[1] + pair.virial[2]) / (3.0 * vol);   // eV/A^3, T = 0
+  };
+  // FIRE (Bitzek et al., PRL 97, 170201 (2006)) on the atoms at fixed box
+  auto relax_atoms = [&](double* pe, double* press) {
+    const int n = s.nlocal;
+    std::vector<double> vel(3 * n, 0.0);
+    double dtf = dt, alpha = 0.1;
+    int npos = 0, it = 0;
+    evaluate(pe, press);
+    for (; it < 20000 && max_force(s) >= ftol; ++it) {
+      double P = 0.0, vn = 0.0, fn = 0.0;
+      for (int k = 0; k < 3 * n; ++k) {
+        P += s.fbuf[k] * vel[k];
+        vn += vel[k] * vel[k];
+        fn += s.fbuf[k] * s.fbuf[k];
+      }
+      vn = std::sqrt(vn);
+      fn = std::sqrt(fn);
+      if (P > 0.0) {
+        for (int k = 0; k < 3 * n; ++k) vel[k] = (1.0 - alpha) * vel[k] + alpha * s.fbuf[k] / fn * vn;
+        if (++npos > 5) {
+          dtf = std::min(dtf * 1.1, 10.0 * dt);
+          alpha *= 0.99;
+        }
+      } else {
+        std::fill(vel.begin(), vel.end(), 0.0);
+        dtf *= 0.5;
+        alpha = 0.1;
+        npos = 0;
+      }
+      const double im = 1.0 / (mass * kMvv2e);
+      for (int k = 0; k < 3 * n; ++k) {
+        vel[k] += dtf * s.fbuf[k] * im;
+        s.xbuf[k] += dtf * vel[k];
+      }
+      evaluate(pe, press);
+    }
+    return it;
+  };
+  double pe = 0.0, press = 0.0;
+  int atom_iters = relax_atoms(&pe, &press);
+  double Lprev = 0.0, Pprev = 0.0;
+  int k = 0;
+  bool converged = false;
+  for (; k < max_box_steps; ++k) {
+    std::printf("relax %d L %.12f %.12f %.12f pe %.12f press_bar %.6f fmax %.3e atom_iters %d\n", k, s.L[0],
+                s.L[1], s.L[2], pe, press * kNktv2p, max_force(s), atom_iters);
+    if (std::fabs(press * kNktv2p) < ptol_bar && max_force(s) < ftol) {
+      converged = true;
+      break;
+    }
+    const double L = s.L[0];
+    double Lnew;
+    if (k == 0) {
+      // first step: a 0.1 % trial strain in the direction of the pressure
+      Lnew = L * (press > 0.0 ? 1.001 : 0.999);
+    } else {
+      Lnew = L - press * (L - Lprev) / (press - Pprev);
+    }
+    Lnew = std::min(std::max(Lnew, 0.98 * L), 1.02 * L);
+    Lprev = L;
+    Pprev = press;
+    const double f = Lnew / L;
+    for (int a = 0; a < 3; ++a) s.L[a] *= f;
+    for (int i = 0; i < s.nlocal; ++i)
+      for (int a = 0; a < 3; ++a) s.xbuf[3 * i + a] *= f;
+    atom_iters = relax_atoms(&pe, &press);
+  }
+  std::printf("{\"mode\": \"boxrelax\", \"atoms\": %d, \"box\": [%.15g, %.15g, %.15g], \"pe\": %.15g, "
+              "\"press_bar\": %.9g, \"fmax\": %.6g, \"box_steps\": %d, \"converged\": %s, "
+              "\"pair_calls\": %lld}\n",
+              s.nlocal, s.L[0], s.L[1], s.L[2], pe, press * kNktv2p, max_force(s), k, converged ? "true" : "false",
+              pair.calls());
+  return converged ? 0 : 3;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
   if (argc < 11) {
     std::fprintf(stderr, "usage: %s data.txt potential.mtp max_atoms max_nbr cutoff mass dt steps every skin "
-                         "[fp64|mixed] [thermo_every] [device|host rows]\n", argv[0]);
+                         "[fp64|mixed] [thermo_every] [device|host rows] [nve|boxrelax] [ftol] [ptol_bar]\n",
+                 argv[0]);
     return 2;
   }
   const std::string data = argv[1], pot = argv[2];
@@ -166,6 +282,14 @@ int main(int argc, char** argv) {
   const std::string prec = argc > 11 ? argv[11] : "fp64";
   const int thermo = argc > 12 ? std::atoi(argv[12]) : 100;
   const std::string rows = argc > 13 ? argv[13] : "device";
+  const std::string mode = argc > 14 ? argv[14] : "nve";
+  const double ftol = argc > 15 ? std::atof(argv[15]) : 1e-6;
+  const double ptol_bar = argc > 16 ? std::atof(argv[16]) : 0.1;
+  const std::string out_path = argc > 17 ? argv[17] : "";
+  if (mode != "nve" && mode != "boxrelax") {
+    std::fprintf(stderr, "unknown mode '%s' (nve or boxrelax)\n", mode.c_str());
+    return 2;
+  }
 
   Sim s;
   {
@@ -244,10 +368,26 @@ int main(int argc, char** argv) {
       const double T = 2.0 * ke / (3.0 * s.nlocal * kBoltz);
       // pressure in bar (LAMMPS metal nktv2p = 1.6021765e6)
       const double press = (2.0 * ke / 3.0 + (pair.virial[0] + pair.virial[1] + pair.virial[2]) / 3.0) / vol * 1.6021765e6;
-      std::printf("step %d pe %.10f ke %.10f etotal %.10f temp %.3f press %.3f\n", step, pe, ke, pe + ke, T, press);
+      std::printf("step %d pe %.10f ke %.10f etotal %.10f temp %.3f press %.6f\n", step, pe, ke, pe + ke, T, press);
       return pe + ke;
     };
 
+    if (mode == "boxrelax") {
+      rc = box_relax(s, pair, rebuild, bind, force_call, mass, dt, steps, ftol, ptol_bar);
+      if (!out_path.empty()) {
+        std::FILE* fo = std::fopen(out_path.c_str(), "w");
+        if (!fo) {
+          std::fprintf(stderr, "cannot write %s\n", out_path.c_str());
+          return 2;
+        }
+        std::fprintf(fo, "%d %d\n%.17g %.17g %.17g\n", s.nlocal, s.ntypes, s.L[0], s.L[1], s.L[2]);
+        for (int i = 0; i < s.nlocal; ++i)
+          std::fprintf(fo, "%d %d %.17g %.17g %.17g 0 0 0\n", s.tag[i], s.type[i], s.xbuf[3 * i], s.xbuf[3 * i + 1],
+                       s.xbuf[3 * i + 2]);
+        std::fclose(fo);
+      }
+      return rc;
+    }
     rebuild();
     bind();
     force_call(1, 1);

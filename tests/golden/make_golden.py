@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden from the reference's own code.
 
-Run in a container that has the reference checkout (read-only) at
-``/root/reference`` (override with ``MTP_REFERENCE``):
+Run with the path of a reference checkout (read-only is fine), given as the
+first argument or in ``MTP_REFERENCE``:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference checkout>
 
 What it does:
 
@@ -45,7 +45,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("MTP_REFERENCE", "/root/reference")
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MTP_REFERENCE")
+if not REF:
+    sys.exit("usage: make_golden.py <reference checkout>  (or set MTP_REFERENCE)")
 sys.path.insert(0, os.path.join(REPO, "jax-mtp_b200"))
 
 from mtp_b200 import synth  # noqa: E402

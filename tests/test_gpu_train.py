@@ -221,3 +221,77 @@ def test_cfg_to_lls_to_lbfgs_pipeline(tmp_path):
     assert all(np.isfinite(hist)) and out["steps"] >= 10
     assert all(b <= a for a, b in zip([L1] + hist[:-1], hist)), hist
     assert hist[-1] < 0.995 * L1, (L0, L1, hist)
+
+
+def _cfg4_batch(nconf, seed):
+    """The first `nconf` configurations of the config-4 generator (32-512 atoms,
+    fcc/bcc/hcp, a in [2.8, 4.2] A, strain 3 %, sigma 0.1 A) whose pairs all lie
+    at or beyond the potential's min_dist.  The generator also makes pairs down
+    to ~1.45 A (fcc near a = 2.8 A with thermal displacement); there the
+    Chebyshev basis is evaluated outside [-1, 1], site energies of this random
+    potential reach ~1e9 eV, and a central difference in FP64 keeps no
+    significant digits, so those configurations are not used for this check."""
+    pot = read_mtp(potential_path("cfg4_L28_S4.mtp"))
+    structs, nds = [], []
+    for s in synth.training_batch(4 * nconf, 32, 512, pot.species_count, seed=seed):
+        nd = synth.build_neighbors(s, pot.max_dist)
+        d = np.linalg.norm(nd.rijs, axis=2)[nd.jtypes >= 0]
+        if d.size and d.min() >= pot.min_dist:
+            structs.append(s)
+            nds.append(nd)
+        if len(nds) == nconf:
+            break
+    assert len(nds) == nconf
+    nd, cfg, offs, vols = synth.pack_batch(nds)
+    return pot, nd, cfg, offs, vols
+
+
+def test_cfg4_adjoint_matches_central_differences():
+    """Config 4's stated gradient check: central differences (h = 1e-6, FP64) of
+    the E/F/stress loss (weights 1, 0.01, 0.001; training/motep_jax_train_function.py:67-74)
+    on 32 random coefficients of the level-28, 4-species potential (2 species,
+    14 radial, 16 basis), over 8 configurations labelled by the potential
+    itself plus the stated noise (1 meV/atom, 10 meV/A, 0.1 GPa)."""
+    pot, nd, cfg, offs, vols = _cfg4_batch(8, seed=81)
+    dev = torch.device("cuda")
+    batch = DeviceBatch.from_numpy(nd, cfg, vols, device=dev)
+    base = {"species": pot.species_coeffs, "radial": pot.radial_coeffs, "basis": pot.moment_coeffs}
+    with MTPEngine(potential_path("cfg4_L28_S4.mtp"), nd.natoms, nd.n_pad) as eng:
+        def predict_np(pp, grad=False):
+            p = {k: torch.tensor(v, dtype=torch.float64, device=dev, requires_grad=grad) for k, v in pp.items()}
+            return p, predict(p, eng, batch)
+
+        with torch.no_grad():
+            _, (E0, F0, S0) = predict_np(base)
+        rng = np.random.default_rng(82)
+        natom_c = torch.as_tensor(np.diff(offs), dtype=torch.float64, device=dev)
+        tt = (E0 + 1e-3 * natom_c * torch.as_tensor(rng.normal(size=E0.shape), device=dev),
+              F0 + 1e-2 * torch.as_tensor(rng.normal(size=F0.shape), device=dev),
+              S0 + 6.2415e-4 * torch.as_tensor(rng.normal(size=S0.shape), device=dev))
+
+        def loss(pp):
+            with torch.no_grad():
+                return float(weighted_loss(*predict_np(pp)[1], tt))
+
+        p, (E, F, S) = predict_np(base, grad=True)
+        L0 = weighted_loss(E, F, S, tt)
+        L0.backward()
+        g = {k: p[k].grad.cpu().numpy() for k in p}
+        L0 = float(L0)
+        eng.sync_status()
+        picks = [("species", (int(i),)) for i in rng.choice(pot.species_count, 2, replace=False)]
+        picks += [("radial", tuple(int(x) for x in rng.integers(0, s))) for s in [pot.radial_coeffs.shape] * 14]
+        picks += [("basis", (int(i),)) for i in rng.choice(pot.alpha_scalar_moments, 16, replace=False)]
+        assert len(picks) == 32
+        h = 1e-6
+        gmax = max(np.abs(v).max() for v in g.values())
+        for key, idx in picks:
+            pp = {k: np.array(v, dtype=np.float64) for k, v in base.items()}
+            pp[key][idx] += h
+            lp = loss(pp)
+            pp[key][idx] -= 2 * h
+            lm = loss(pp)
+            fd = (lp - lm) / (2 * h)
+            # 1e-6 relative to the component, or to the gradient's scale for
+            # components near zero (FP64 roundoff of the loss over 2h)
+            assert abs(fd - g[key][idx]) <= 1e-6 * max(abs(fd), 1e-3 * gmax), (key, idx, fd, g[key][idx], gmax)

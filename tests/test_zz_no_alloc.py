@@ -76,8 +76,19 @@ def test_noalloc_rejects_inputs_above_its_limits():
             eng.compute_device_noalloc(it, rij, js, js, cnt, E, F, W)
         assert ei.value.code == 3
         assert "allocation-free limit" in str(ei.value)
-        # too many slots for the fixed scratch, with few atoms
-        m = _lib.NOALLOC_MAX_SLOTS // 16 + 1
+    # too many neighbour slots for the fixed scratch, with an atom count under
+    # the atom limit: 8,193 atoms x 32 slots = 262,176 > MTP_NOALLOC_MAX_SLOTS
+    m, stride = _lib.NOALLOC_MAX_SLOTS // 32 + 1, 32
+    assert m <= _lib.NOALLOC_MAX_ATOMS and m * stride > _lib.NOALLOC_MAX_SLOTS
+    with MTPEngine(path, m, stride) as eng:
+        it = torch.zeros(m, dtype=torch.int32, device=dev)
+        rij = torch.zeros((m, stride, 3), dtype=torch.float64, device=dev)
+        js = torch.full((m, stride), -1, dtype=torch.int32, device=dev)
+        cnt = torch.zeros(m, dtype=torch.int32, device=dev)
+        E = torch.zeros(1, dtype=torch.float64, device=dev)
+        F = torch.zeros((m, 3), dtype=torch.float64, device=dev)
+        W = torch.zeros(6, dtype=torch.float64, device=dev)
         with pytest.raises(_lib.MTPError) as ei:
-            eng.compute_device_noalloc(it[:m], rij[:m], js[:m], js[:m], cnt[:m], E, F[:m], W)
+            eng.compute_device_noalloc(it, rij, js, js, cnt, E, F, W)
         assert ei.value.code == 3
+        assert "neighbour slots" in str(ei.value)

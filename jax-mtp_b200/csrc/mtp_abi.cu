@@ -80,6 +80,7 @@ struct mtp_handle {
   double *d_radial = nullptr, *d_species = nullptr, *d_theta = nullptr, *d_seed_val = nullptr;
   int *d_mapping = nullptr, *d_seed_idx = nullptr, *d_zero = nullptr, *d_abc = nullptr, *d_mk = nullptr;
   int* d_dense_k = nullptr;
+  int* d_dm_pos = nullptr;   // Schedule::dm_pos (the same for every schedule of the potential)
   int nseed = 0;
   // input / output / scratch buffers sized by the capacities
   int *d_itypes = nullptr, *d_js = nullptr, *d_jtypes = nullptr, *d_counts = nullptr;
@@ -179,6 +180,7 @@ DevModel make_model(mtp_handle* h, const DeviceSchedule& ds) {
   md.mono_abc = h->d_abc;
   md.mono_k = h->d_mk;
   md.dense_k = h->d_dense_k;
+  md.dm_pos = h->d_dm_pos;
   md.Q = s.Q;
   md.npairs = s.npairs;
   md.tri = s.tri ? 1 : 0;
@@ -228,6 +230,9 @@ int get_schedule(mtp_handle* h, int lanes, int width, DeviceSchedule** out) {
       MTP_CUDA(h, dalloc(&h->d_dense_k, ds.sched.dense_k.size()));
       MTP_CUDA(h, cudaMemcpy(h->d_dense_k, ds.sched.dense_k.data(), ds.sched.dense_k.size() * sizeof(int),
                              cudaMemcpyHostToDevice));
+      MTP_CUDA(h, dalloc(&h->d_dm_pos, ds.sched.dm_pos.size()));
+      MTP_CUDA(h, cudaMemcpy(h->d_dm_pos, ds.sched.dm_pos.data(), ds.sched.dm_pos.size() * sizeof(int),
+                             cudaMemcpyHostToDevice));
       MTP_CUDA(h, dalloc(&h->d_zero, ds.sched.zero_list.size()));
       if (!ds.sched.zero_list.empty())
         MTP_CUDA(h, cudaMemcpy(h->d_zero, ds.sched.zero_list.data(), ds.sched.zero_list.size() * sizeof(int),
@@ -247,6 +252,10 @@ int upload_coeffs(mtp_handle* h) {
   std::vector<int> si;
   std::vector<double> sv;
   seed_list(p, si, sv);
+  // seeds go to the adjoint positions of their moments
+  std::vector<int> dm_pos;
+  adjoint_layout(p, dm_pos);
+  for (int& k : si) k = dm_pos[k];
   h->nseed = static_cast<int>(si.size());
   MTP_CUDA(h, cudaMemcpy(h->d_seed_idx, si.data(), si.size() * sizeof(int), cudaMemcpyHostToDevice));
   MTP_CUDA(h, cudaMemcpy(h->d_seed_val, sv.data(), sv.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -258,7 +267,7 @@ void free_handle(mtp_handle* h) {
   auto F = [](void* p) { if (p) cudaFree(p); };
   for (auto& kv : h->scheds) F(kv.second.d_entries);
   F(h->d_radial); F(h->d_species); F(h->d_theta); F(h->d_seed_val);
-  F(h->d_mapping); F(h->d_seed_idx); F(h->d_zero); F(h->d_abc); F(h->d_mk); F(h->d_dense_k);
+  F(h->d_mapping); F(h->d_seed_idx); F(h->d_zero); F(h->d_abc); F(h->d_mk); F(h->d_dense_k); F(h->d_dm_pos);
   F(h->d_itypes); F(h->d_js); F(h->d_jtypes); F(h->d_counts); F(h->d_rijs);
   F(h->d_G); F(h->d_E); F(h->d_F); F(h->d_wown); F(h->d_vatom);
   F(h->d_in_cnt); F(h->d_in_ptr); F(h->d_in_cursor); F(h->d_in_slot); F(h->d_blk);
@@ -677,7 +686,7 @@ int mtp_schedule_emulate(const char* path, int lanes, int width, const double* b
   double e = emulate_schedule(pot, s, V);
   for (int k = 0; k < pot.M; ++k) {
     moments[k] = V[s.v_m + k];
-    dmoments[k] = V[s.v_dm + k];
+    dmoments[k] = V[s.v_dm + s.dm_pos[k]];
   }
   if (energy_part) *energy_part = e;
   return MTP_OK;

@@ -64,7 +64,9 @@ struct DevModel {
   int nseed, nzero;
   int S, R, K, M, B, P, D, Sa;
   int Q, npairs;
-  int tri;                  // Schedule::tri: step k of a force-phase chain has k / 2 + 1 radial functions
+  int tri;                  // Schedule::tri: step k of a force-phase chain has k / 2 + 1 radial functions,
+                            // and the basic moments' adjoints are in chain order (dm_pos)
+  const int* dm_pos;        // [M] adjoint position of each moment (Schedule::dm_pos)
   int nmu[kMaxDegree + 1];  // radial functions with a basic moment of each degree
   int v_m, v_dm, v_zero, v_one, v_size;
   double scaling, rmin, rmax;
@@ -280,12 +282,15 @@ __device__ __forceinline__ void stream_entries_n(const uint2* __restrict__ ent, 
 // side by side.  The tpn threads of a neighbour pair take the (a, b)
 // pairs in snake order (sl, 2 tpn-1-sl, 2 tpn+sl, ...) of the pair order
 // (a + b ascending), so their shares differ by one pair at most.
-// kTri (Schedule::tri): the chain's step k = top - c has table entries for
-// mu <= k / 2 only (the others are zero); the chain is unrolled over k so each
-// step does exactly those multiply-adds (level 24: 581 of the dense table's
-// 1,716 (slot, mu) entries).  The sums keep the dense order with the zero
-// terms left out.
-template <typename T, int R, bool kTwo, bool kTri>
+// kTri (Schedule::tri): the chain's step k = top - c has the radial functions
+// mu <= k / 2 only; the chain is unrolled over k so each step does exactly
+// those multiply-adds (level 24: 581 of a dense table's 1,716 (slot, mu)
+// entries), and dmt is the atom's adjoint region in the value space (element
+// stride AS, the block's atoms), whose basic moments are stored in chain order:
+// a pair of diagonal s = a + b starts floor((D - s + 2)^2 / 4) after the
+// previous pair of its diagonal and step k at floor((k + 1)^2 / 4) within it.
+// Otherwise dmt is the dense table [slot][R] in pair order.
+template <typename T, int R, bool kTwo, bool kTri, int AS>
 __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
                                         int npairs, int D1, const T* __restrict__ fq0, const T* __restrict__ fpq0,
                                         const T* __restrict__ fq1, const T* __restrict__ fpq1, bool two,
@@ -302,25 +307,27 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
   // diagonal s = a + b of the current pair, its first pair index, and the
   // first dense slot of the diagonal (pair order: each pair of diagonal s
   // owns D - s + 1 slots, so slot bases follow without a table lookup)
-  int s = 0, sb = 0, slot_sb = 0;
+  int s = 0, sb = 0, slot_sb = 0, cb_sb = 0;
   for (int k = 0;; ++k) {
     const int i = (k >> 1) * 2 * tpn + ((k & 1) ? 2 * tpn - 1 - sl : sl);
     if (i >= npairs) break;
     while (i >= sb + s + 1) {
       sb += s + 1;
       slot_sb += (s + 1) * (D - s + 1);
+      cb_sb += (s + 1) * (((D - s + 2) * (D - s + 2)) >> 2);
       ++s;
     }
     const int ea = i - sb, eb = s - ea, top = D - s;
-    const T* drow = dmt + (slot_sb + ea * (D - s + 1) + top) * R;
+    const T* drow = kTri ? dmt + (cb_sb + ea * (((top + 2) * (top + 2)) >> 2)) * AS
+                         : dmt + (slot_sb + ea * (D - s + 1) + top) * R;
     T h0 = T(0), hz0 = T(0), hs0 = T(0), h1 = T(0), hz1 = T(0), hs1 = T(0);
     // one Horner step: table row drow, radial functions mu < nm
-    auto step = [&](const T* row, int nm) {
+    auto step = [&](const T* row, int nm, int stride) {
       T w0 = T(0), wp0 = T(0), w1 = T(0), wp1 = T(0);
 #pragma unroll
       for (int mu = 0; mu < R; ++mu) {
         if (mu < nm) {
-          const T g = row[mu];
+          const T g = row[mu * stride];
           w0 = dev_fma(g, f0[mu], w0);
           wp0 = dev_fma(g, fp0[mu], wp0);
           if (kTwo) {
@@ -342,11 +349,11 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
 #pragma unroll
       for (int k = 0; k <= kMaxDegree; ++k) {
         if (k > top) break;
-        step(drow - k * R, k / 2 + 1);
+        step(drow + (((k + 1) * (k + 1)) >> 2) * AS, k / 2 + 1, AS);
       }
     } else {
 #pragma unroll 1
-      for (int c = top; c >= 0; --c, drow -= R) step(drow, R);
+      for (int c = top; c >= 0; --c, drow -= R) step(drow, R, 1);
     }
     {
       const T xa = pw0[ea], yb = pw0[D1 + eb];
@@ -691,16 +698,20 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
     }
 
     // ---- N3: dE_i/dr_ij per kept neighbour -------------------------------
-    // dense table Dm[a][slot][mu] = dE/dm of basic moment (mu, slot) over the
-    // full monomial simplex in pair order (0 where the basis has no moment)
+    // level-structured bases read the basic moments' adjoints in place (chain
+    // order); otherwise a dense table Dm[a][slot][mu] = dE/dm of basic moment
+    // (mu, slot) over the full monomial simplex in pair order (0 where the
+    // basis has no moment) is filled first
     T* sDm = L.dmt_in_v ? V + md.v_m * A : reinterpret_cast<T*>(smem + L.dmt);
     const int QR = md.Q * R;
-    for (int x = tid; x < QR * A; x += NT) {
-      const int a = x / QR, r = x - a * QR;
-      const int k = __ldg(md.dense_k + (r / R) * kMaxR + r % R);
-      sDm[x] = k >= 0 ? V[(md.v_dm + k) * A + a] : T(0);
+    if (!md.tri) {
+      for (int x = tid; x < QR * A; x += NT) {
+        const int a = x / QR, r = x - a * QR;
+        const int k = __ldg(md.dense_k + (r / R) * kMaxR + r % R);
+        sDm[x] = k >= 0 ? V[(md.v_dm + __ldg(md.dm_pos + k)) * A + a] : T(0);
+      }
+      __syncthreads();
     }
-    __syncthreads();
 #pragma unroll
     for (int a = 0; a < A; ++a) {
       const int atom = base + a;
@@ -728,17 +739,17 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
         const int sl = idx & (tpn - 1);
         T Ssum[2] = {T(0), T(0)}, Gx[2] = {T(0), T(0)}, Gy[2] = {T(0), T(0)}, Gz[2] = {T(0), T(0)};
         if (active) {
-          const T* dmt = sDm + static_cast<size_t>(a) * QR;
+          const T* dmt = md.tri ? V + static_cast<size_t>(md.v_dm) * A + a : sDm + static_cast<size_t>(a) * QR;
           const int qb = two ? q1 : q0;
           switch (R) {
 #define MTP_N3_CASE(RR)                                                                                        \
   case RR:                                                                                                     \
     if (md.tri)                                                                                                \
-      n3_sums<T, RR, kTwoN, true>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R,          \
+      n3_sums<T, RR, kTwoN, true, A>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R,          \
                                   sFp + qb * R, two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2],          \
                                   sU[4 * qb + 2], sl, tpn, Ssum, Gx, Gy, Gz);                                 \
     else                                                                                                       \
-      n3_sums<T, RR, kTwoN, false>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R,         \
+      n3_sums<T, RR, kTwoN, false, 1>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R,         \
                                    sFp + qb * R, two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2],         \
                                    sU[4 * qb + 2], sl, tpn, Ssum, Gx, Gy, Gz);                                \
     break;

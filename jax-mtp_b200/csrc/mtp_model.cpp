@@ -2,6 +2,7 @@
 #include "mtp_model.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cctype>
 #include <climits>
 #include <cmath>
@@ -408,6 +409,37 @@ void emit_jobs(const std::vector<Job>& jobs, int lanes, int width, bool allow_sw
 
 }  // namespace
 
+bool adjoint_layout(const Potential& pot, std::vector<int>& dm_pos) {
+  const int M = pot.M, B = pot.B;
+  dm_pos.resize(M);
+  for (int k = 0; k < M; ++k) dm_pos[k] = k;
+  if (B == 0) return false;
+  int D = 0;
+  std::map<std::array<int, 4>, int> basic_of;
+  for (int k = 0; k < B; ++k) {
+    const int* r = &pot.basic[4 * k];
+    D = std::max(D, r[1] + r[2] + r[3]);
+    basic_of[{r[0], r[1], r[2], r[3]}] = k;
+  }
+  std::vector<int> pos(B, -1);
+  int next = 0;
+  for (int sum = 0; sum <= D; ++sum) {
+    for (int a = 0; a <= sum; ++a) {
+      const int b = sum - a, top = D - sum;
+      for (int k = 0; k <= top; ++k) {
+        for (int mu = 0; mu <= k / 2; ++mu) {
+          auto it = basic_of.find({mu, a, b, top - k});
+          if (it == basic_of.end()) return false;   // a hole: not level-structured
+          pos[it->second] = next++;
+        }
+      }
+    }
+  }
+  if (next != B) return false;                      // basic moments outside the pattern
+  for (int k = 0; k < B; ++k) dm_pos[k] = pos[k];
+  return true;
+}
+
 void seed_list(const Potential& pot, std::vector<int>& idx, std::vector<double>& val) {
   std::map<int, double> acc;
   for (int a = 0; a < pot.Sa; ++a) acc[pot.mapping[a]] += pot.moment[a];
@@ -513,11 +545,7 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
       }
     }
   }
-  s.tri = true;
-  for (int k = 0; k < B; ++k) {
-    const int deg = pot.basic[4 * k + 1] + pot.basic[4 * k + 2] + pot.basic[4 * k + 3];
-    if (2 * pot.basic[4 * k] > s.D - deg) s.tri = false;
-  }
+  s.tri = adjoint_layout(pot, s.dm_pos);
   // moments that are read but never written stay zero for the whole run
   std::vector<char> read(M, 0);
   for (int e = 0; e < T; ++e) { read[pot.times[4 * e]] = 1; read[pot.times[4 * e + 1]] = 1; }
@@ -551,11 +579,11 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
     auto it = job_of.find(src);
     if (it == job_of.end()) {
       job_of[src] = static_cast<int>(jobs.size());
-      jobs.push_back(Job{static_cast<uint32_t>(s.v_dm + src), kOpAdd, {}});
+      jobs.push_back(Job{static_cast<uint32_t>(s.v_dm + s.dm_pos[src]), kOpAdd, {}});
       it = job_of.find(src);
     }
-    jobs[it->second].sides.push_back(
-        Side{static_cast<uint32_t>(s.v_dm + tgt), static_cast<uint32_t>(s.v_m + other), static_cast<uint32_t>(mult)});
+    jobs[it->second].sides.push_back(Side{static_cast<uint32_t>(s.v_dm + s.dm_pos[tgt]),
+                                          static_cast<uint32_t>(s.v_m + other), static_cast<uint32_t>(mult)});
   };
   for (int L = maxd; L >= 1; --L) {
     std::vector<Job> jobs;
@@ -670,7 +698,7 @@ double emulate_schedule(const Potential& pot, const Schedule& s, std::vector<dou
   std::vector<int> si;
   std::vector<double> sv;
   seed_list(pot, si, sv);
-  for (size_t i = 0; i < si.size(); ++i) V[s.v_dm + si[i]] = sv[i];
+  for (size_t i = 0; i < si.size(); ++i) V[s.v_dm + s.dm_pos[si[i]]] = sv[i];
   for (const Pass& p : s.rev) run(p);
   return e;
 }

@@ -88,11 +88,14 @@ struct Schedule {
   int Q = 0;                    // (D+1)(D+2)(D+3)/6 slots
   int npairs = 0;               // (D+1)(D+2)/2 pairs
   std::vector<int> dense_k;     // [Q][kMaxR] basic-moment index of slot and mu, or -1
-  // Every basic moment (mu, a, b, c) has 2 mu <= D - (a + b + c): the radial
-  // function mu only meets monomials of degree <= D - 2 mu (true of every
-  // level-defined MTP basis).  Then a force-phase Horner step k = D - degree
-  // has nonzero table entries for mu <= k / 2 only.
+  // Level-structured basis (adjoint_layout): radial function mu meets exactly
+  // the monomials of degree <= D - 2 mu.  Then a force-phase Horner step
+  // k = D - degree has the radial functions mu <= k / 2, and the adjoints of
+  // the basic moments are laid out in that chain order (dm_pos), so the force
+  // phase reads them in place.
   bool tri = false;
+  // dE/dm of moment k lives at v_dm + dm_pos[k] (a permutation of [0, M))
+  std::vector<int> dm_pos;
   std::vector<int> zero_list;   // non-basic moments never written (must read as 0)
   std::vector<Pass> fwd, rev;   // passes in execution order
   std::vector<uint32_t> entries;  // pairs (x, y) per entry: 2 words; kStepAlign no-op rows at the end
@@ -110,6 +113,18 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& out, std::string&
 // in V[v_m .. v_m + B) set.  Fills moments, adjoints (seeded with moment
 // coefficients), and returns sum_alpha theta_alpha m[map_alpha].
 double emulate_schedule(const Potential& pot, const Schedule& s, std::vector<double>& V);
+
+// Position of every moment's adjoint within the adjoint region (dm_pos, a
+// permutation of [0, M)); returns whether the basis is level-structured:
+// every basic moment (mu, a, b, c) has 2 mu <= D - (a + b + c) and every such
+// (mu, monomial) is a basic moment.  Then the basic moments' adjoints take
+// positions [0, B) in force-phase chain order: monomial pairs (a, b) by
+// a + b, then a; within a pair k = D - a - b - c = 0 .. D - a - b, and within
+// a step mu = 0 .. k / 2, so step k of a pair starts floor((k + 1)^2 / 4)
+// after the pair's first position and a pair of s = a + b holds
+// floor((D - s + 2)^2 / 4).  Otherwise (and for every non-basic moment)
+// dm_pos[k] = k.
+bool adjoint_layout(const Potential& pot, std::vector<int>& dm_pos);
 
 // Seeds of the reverse pass: unique moments of the mapping with summed theta.
 void seed_list(const Potential& pot, std::vector<int>& idx, std::vector<double>& val);

@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
               if (mu < R) {
                 const int k = __ldg(md.mono_k + kMaxR * p + mu);
                 if (k >= 0) {
-                  const T2 lt = V[md.v_dm + k];   // (lambda, tau)
+                  const T2 lt = V[md.v_dm + __ldg(md.dm_pos + k)];   // (lambda, tau)
                   GA[mu] = dev_fma(lt.x, mono, dev_fma(lt.y, dmono, GA[mu]));
                   GB[mu] = dev_fma(lt.y, mono, GB[mu]);
                 }

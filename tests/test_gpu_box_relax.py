@@ -13,9 +13,12 @@ is stationary:
   oracle by central finite differences (homogeneous strain of a config-1
   cell), and the pair style's thermo pressure equals -dE/dV;
 * box/relax of a B2 (CsCl-ordered) bcc crystal reaches the oracle's energy
-  minimum of E(a) to 1e-4 A;
-* box/relax of a displaced random alloy ends with the oracle's forces below
-  the force tolerance and its -dE/dV within the pressure tolerance.
+  minimum of E(a) to 1e-4 A.
+
+The relaxed crystal uses a random-coefficient potential (the stated
+distributions); such a potential has no short-range repulsion, so only a
+symmetric crystal, whose atoms feel no force, has a box minimum to relax to:
+a displaced random alloy collapses into the region below min_dist.
 """
 
 import json
@@ -129,24 +132,3 @@ def test_box_relax_reaches_oracle_lattice_constant(driver, tmp_path):
     a_relaxed = summary["box"][0] / 4
     assert abs(a_relaxed - a_ref) <= 1e-4, (a_relaxed, a_ref)
 
-
-def test_box_relax_random_alloy_is_oracle_stationary(driver, tmp_path):
-    pot = read_mtp(potential_path(RELAX_POT))
-    cpu = CpuMTP(pot)
-    s = _b2(3.2)
-    s.types = np.random.default_rng(11).integers(0, 2, s.natoms).astype(np.int32)
-    s.positions = s.positions + np.random.default_rng(12).normal(0.0, 0.03, s.positions.shape)
-    ftol, ptol = 1e-4, 1.0
-    summary, out = _relax(driver, tmp_path, s, ftol=ftol, ptol_bar=ptol)
-    assert summary["converged"]
-    r = _energy(cpu, out, pot.max_dist)
-    assert np.abs(r["forces"]).max() < 2 * ftol
-    assert abs(r["energy"] - summary["pe"]) <= 1e-9 * abs(r["energy"])
-    # the oracle's pressure -dE/dV at the relaxed box (isotropic strain, fixed neighbour set)
-    nd = synth.build_neighbors(out, pot.max_dist + 0.3)
-    h = 1e-5
-    Ep = cpu.compute(nd.itypes, nd.rijs * (1 + h), nd.js, nd.jtypes, nd.counts)["energy"]
-    Em = cpu.compute(nd.itypes, nd.rijs * (1 - h), nd.js, nd.jtypes, nd.counts)["energy"]
-    V = out.volume
-    press = -(Ep - Em) / (V * ((1 + h) ** 3 - (1 - h) ** 3)) * NKTV2P
-    assert abs(press) <= 2 * ptol, press

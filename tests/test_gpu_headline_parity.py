@@ -89,7 +89,8 @@ def test_benchmark_potential_mixed_absolute_bars(name, threads, apb):
         eng.set_launch(threads, 0, apb)
         out = eng.compute(nd.itypes, nd.rijs, nd.js, nd.jtypes, nd.counts, eatom=True)
         ran = eng.launch()
-    assert (ran["threads"], ran["atoms_per_block"]) == (threads, apb)
+    # the engine may narrow the lanes where that fits more blocks per SM (level 16)
+    assert ran["atoms_per_block"] == apb and ran["threads"] in (threads, 256, 128)
     de_site = np.abs(out["site_energies"] - ref["site_energies"]).max() * 1e3
     de_total = abs(out["energy"] - ref["energy"]) / N * 1e3
     df = np.abs(out["forces"] - ref["forces"]).max() * 1e3

@@ -624,14 +624,19 @@ def run_train(args, device, dist):
     E_t = E_l + 1e-3 * natom_c * torch.randn(batch.nconfig, generator=g, dtype=torch.float64).to(device)
     F_t = F_l + 1e-2 * torch.randn(F_l.shape, generator=g, dtype=torch.float64).to(device)
     S_t = S_l + 6.2415e-4 * torch.randn(S_l.shape, generator=g, dtype=torch.float64).to(device)
-    with MTPEngine(os.path.join(potdir, "cfg3_L20_S2.mtp"), nd.natoms, nd.n_pad, precision="mixed") as eng3:
+    from mtp_b200.autotune import tile_candidates, tune_batch, tune_step
+    tiles3 = tile_candidates(int(nd.counts.max()))
+    with MTPEngine(os.path.join(potdir, "cfg3_L20_S2.mtp"), nd.natoms, max(tiles3), precision="mixed") as eng3:
+        # neighbour tile, threads and atoms per block by the autotuner, on this batch
+        tuned3 = tune_batch(eng3, batch, tiles=tiles3)
+        b3 = tuned3["batch"]
+
         def fwd3():
-            eng3.batch_device(batch.itypes, batch.rijs, batch.js, batch.jtypes, batch.counts, batch.cfg,
-                              batch.volumes, batch.nconfig)
+            eng3.batch_device(b3.itypes, b3.rijs, b3.js, b3.jtypes, b3.counts, b3.cfg, b3.volumes, b3.nconfig)
         steps = max(3, min(args.steps, 10))
         ms = timed(fwd3, steps, 3)
-        E_p, F_p, S_p = eng3.batch_device(batch.itypes, batch.rijs, batch.js, batch.jtypes, batch.counts, batch.cfg,
-                                          batch.volumes, batch.nconfig)
+        E_p, F_p, S_p = eng3.batch_device(b3.itypes, b3.rijs, b3.js, b3.jtypes, b3.counts, b3.cfg, b3.volumes,
+                                          b3.nconfig)
         loss = float(weighted_loss(E_p, F_p, S_p, (E_t, F_t, S_t)))
         rmse3 = rmse_per_atom(E_p, F_p, E_t, F_t, natom_c)
         eng3.sync_status()
@@ -655,8 +660,12 @@ def run_train(args, device, dist):
                              "rmse_before": rmse3, "rmse_after": rmse_fit,
                              "rows": int(batch.nconfig * 7 + 3 * batch.natoms)}
     out["cfg3_batched_forward"] = {"value": world * batch.nconfig * steps / (ms * 1e-3), "unit": "cfg/s",
-                                   "configs": batch.nconfig, "atoms": batch.natoms, "nbr_stride": nd.n_pad,
+                                   "configs": batch.nconfig, "atoms": batch.natoms, "nbr_stride": b3.stride,
                                    "ms_per_batch": ms / steps, "precision": "mixed", "loss_vs_labels": loss,
+                                   "autotuned": {"n_pad": tuned3["n_pad"], "threads": tuned3["threads"],
+                                                 "atoms_per_block": tuned3["atoms_per_block"],
+                                                 "candidates_ms": {k: (v["ms"] if isinstance(v, dict) else v)
+                                                                   for k, v in tuned3["timings"].items()}},
                                    "rmse_vs_labels": rmse3, "data_diagnostics": diag3,
                                    "labels": "second random level-20 MTP (seed 7) + noise 1 meV/atom, "
                                              "10 meV/A, 0.1 GPa",
@@ -671,7 +680,8 @@ def run_train(args, device, dist):
     diag4 = batch_diagnostics(nds, pot4.min_dist)
     nd, cfg, offs, vols = synth.pack_batch(nds)
     batch = DeviceBatch.from_numpy(nd, cfg, vols, device=device)
-    with MTPEngine(os.path.join(potdir, "cfg4_L28_S4.mtp"), nd.natoms, nd.n_pad, precision="fp64") as eng4:
+    tiles4 = tile_candidates(int(nd.counts.max()))
+    with MTPEngine(os.path.join(potdir, "cfg4_L28_S4.mtp"), nd.natoms, max(tiles4), precision="fp64") as eng4:
         params = {k: torch.tensor(v, dtype=torch.float64, device=device, requires_grad=True)
                   for k, v in (("species", pot4.species_coeffs), ("basis", pot4.moment_coeffs),
                                ("radial", pot4.radial_coeffs))}
@@ -682,21 +692,30 @@ def run_train(args, device, dist):
                F0 + 1e-2 * torch.randn(F0.shape, generator=g, dtype=torch.float64).to(device),
                S0 + 6.2415e-4 * torch.randn(S0.shape, generator=g, dtype=torch.float64).to(device))
 
-        def step4():
+        def step_on(b):
             for v in params.values():
                 v.grad = None
-            L = weighted_loss(*predict(params, eng4, batch), tgt)
+            L = weighted_loss(*predict(params, eng4, b), tgt)
             L.backward()
 
+        # neighbour tile, threads and atoms per block of the whole step (the
+        # forward and the adjoint share the engine's launch settings)
+        tuned4 = tune_step(eng4, batch, step_on, candidates=((256, 1), (512, 1), (256, 2), (512, 2)), tiles=tiles4,
+                           calls=1, tag="train_step")
+        b4 = tuned4["batch"]
         steps = max(2, min(args.steps, 4))
-        ms = timed(step4, steps, 1)
+        ms = timed(lambda: step_on(b4), steps, 1)
         eng4.sync_status()
     out["cfg4_train_step"] = {"value": world * batch.nconfig * steps / (ms * 1e-3), "unit": "cfg/s",
-                              "configs": batch.nconfig, "atoms": batch.natoms, "nbr_stride": nd.n_pad,
+                              "configs": batch.nconfig, "atoms": batch.natoms, "nbr_stride": b4.stride,
                               "ms_per_step": ms / steps, "precision": "fp64",
                               "step": "batched forward (E, F, stress) + loss + hand-written adjoint w.r.t. all "
                                       "coefficients", "jax_grad_baseline": "unavailable on this box (no JAX)",
-                              "data_diagnostics": diag4}
+                              "data_diagnostics": diag4,
+                              "autotuned": {"n_pad": tuned4["n_pad"], "threads": tuned4["threads"],
+                                            "atoms_per_block": tuned4["atoms_per_block"],
+                                            "candidates_ms": {k: (v["ms"] if isinstance(v, dict) else v)
+                                                              for k, v in tuned4["timings"].items()}}}
     return out
 
 

@@ -54,6 +54,28 @@ class DeviceBatch:
     def natoms(self) -> int:
         return int(self.itypes.shape[0])
 
+    @property
+    def stride(self) -> int:
+        return int(self.rijs.shape[1])
+
+    def with_stride(self, n: int) -> "DeviceBatch":
+        """The same batch with rows of `n` slots (every row's count must fit;
+        slots past a row's count are never read, so narrowing drops padding only)."""
+        longest = int(self.counts.max()) if self.natoms else 0
+        if n <= 0 or n < longest:
+            raise ValueError(f"rows of {n} slots cannot hold the longest row ({longest})")
+        if n <= self.stride:
+            sl = slice(0, n)
+            return dataclasses.replace(self, rijs=self.rijs[:, sl].contiguous(), js=self.js[:, sl].contiguous(),
+                                       jtypes=self.jtypes[:, sl].contiguous())
+        pad = n - self.stride
+        N = self.natoms
+        dev = self.rijs.device
+        return dataclasses.replace(
+            self, rijs=torch.cat([self.rijs, torch.zeros((N, pad, 3), dtype=self.rijs.dtype, device=dev)], 1),
+            js=torch.cat([self.js, torch.full((N, pad), -1, dtype=self.js.dtype, device=dev)], 1),
+            jtypes=torch.cat([self.jtypes, torch.full((N, pad), -1, dtype=self.jtypes.dtype, device=dev)], 1))
+
 
 class MTPFunction(torch.autograd.Function):
     """(species, moment, radial) -> (E [C], F [N,3], sigma [C,6])."""

@@ -299,3 +299,40 @@ def test_cfg4_adjoint_matches_central_differences():
             # 1e-6 relative to the component, or to the gradient's scale for
             # components near zero (FP64 roundoff of the loss over h)
             assert abs(fd - g[key][idx]) <= 1e-6 * max(abs(fd), 1e-3 * gmax), (key, idx, fd, g[key][idx], gmax)
+
+
+def test_autotuned_training_launches_agree():
+    """The training autotuner (neighbour tile, threads, atoms per block) changes
+    only the launch: the tuned batched forward and the tuned training gradient
+    equal the untuned ones (FP64, <= 1e-10 relative)."""
+    from mtp_b200.autotune import tile_candidates, tune_batch, tune_step
+    name = "cfg3_L20_S2.mtp"
+    pot, nd, cfg, vols, targets = _setup(name, 4, 8, 40, seed=91)
+    dev = torch.device("cuda")
+    batch = DeviceBatch.from_numpy(nd, cfg, vols, device=dev)
+    tt = tuple(torch.as_tensor(t, dtype=torch.float64, device=dev) for t in targets)
+    tiles = tile_candidates(int(nd.counts.max()))
+    base = {"species": pot.species_coeffs, "radial": pot.radial_coeffs, "basis": pot.moment_coeffs}
+    with MTPEngine(potential_path(name), nd.natoms, max(tiles)) as eng:
+        def grads(b):
+            p = {k: torch.tensor(v, dtype=torch.float64, device=dev, requires_grad=True) for k, v in base.items()}
+            L = weighted_loss(*predict(p, eng, b), tt)
+            L.backward()
+            return [p[k].grad.cpu().numpy() for k in ("species", "radial", "basis")]
+
+        E0, F0, S0 = eng.batch_device(batch.itypes, batch.rijs, batch.js, batch.jtypes, batch.counts, batch.cfg,
+                                      batch.volumes, batch.nconfig)
+        g0 = grads(batch)
+        r = tune_batch(eng, batch, tiles=tiles, calls=1)
+        b = r["batch"]
+        assert r["n_pad"] in tiles and b.stride == r["n_pad"] and len(r["timings"]) >= len(tiles)
+        E1, F1, S1 = eng.batch_device(b.itypes, b.rijs, b.js, b.jtypes, b.counts, b.cfg, b.volumes, b.nconfig)
+        r2 = tune_step(eng, batch, lambda bb: grads(bb), candidates=((256, 1), (512, 1), (256, 2)), tiles=tiles,
+                       calls=1)
+        g1 = grads(r2["batch"])
+        eng.sync_status()
+    assert _rel(E1.cpu().numpy(), E0.cpu().numpy()) <= 1e-10
+    assert _rel(F1.cpu().numpy(), F0.cpu().numpy()) <= 1e-10
+    assert _rel(S1.cpu().numpy(), S0.cpu().numpy()) <= 1e-10
+    for a, c in zip(g1, g0):
+        assert _rel(a, c) <= 1e-10

@@ -141,3 +141,31 @@ def test_ghosts_and_lists_reject_small_or_skewed_cells():
     h = synth.lattice_structure("hcp", 3.0, (3, 3, 3))
     with pytest.raises(ValueError):
         synth.ghosts_and_lists(h, 5.0)
+
+
+def test_tile_candidates_and_batch_restride():
+    """Neighbour-tile candidates of the training autotuner, and a batch restrided
+    to a tile keeps every row's real slots (only padding changes)."""
+    from mtp_b200.autotune import tile_candidates
+    from mtp_b200.train import DeviceBatch
+    assert tile_candidates(90) == (96,)
+    assert tile_candidates(100) == (104, 112, 128)
+    assert tile_candidates(130) == (136, 144, 160)
+    assert tile_candidates(64) == (64,)
+    pot = read_mtp(potential_path("cfg3_L20_S2.mtp"))
+    structs = synth.training_batch(3, 8, 20, pot.species_count, seed=3)
+    nds = [synth.build_neighbors(s, pot.max_dist) for s in structs]
+    nd, cfg, offs, vols = synth.pack_batch(nds)
+    b = DeviceBatch.from_numpy(nd, cfg, vols, device="cpu")
+    longest = int(b.counts.max())
+    for n in (longest, b.stride + 16):
+        r = b.with_stride(n)
+        assert r.stride == n
+        for i in range(b.natoms):
+            c = int(b.counts[i])
+            assert torch.equal(r.rijs[i, :c], b.rijs[i, :c])
+            assert torch.equal(r.js[i, :c], b.js[i, :c])
+            assert torch.equal(r.jtypes[i, :c], b.jtypes[i, :c])
+        assert bool((r.jtypes[:, b.stride:] == -1).all()) if n > b.stride else True
+    with pytest.raises(ValueError):
+        b.with_stride(longest - 1)

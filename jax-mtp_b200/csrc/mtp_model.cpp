@@ -267,7 +267,7 @@ struct RawPass {
 // that adds the fewest conflicts, and the last entry of a job carries its
 // flush.
 RawPass lay_out(const std::vector<Job>& jobs, int lanes, int width, bool allow_swap) {
-  constexpr size_t kWindow = 32;
+  constexpr size_t kWindow = 64;
   std::vector<int> order(jobs.size());
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(),

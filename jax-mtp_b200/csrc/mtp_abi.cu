@@ -33,6 +33,8 @@ std::string g_create_error;
 struct DeviceSchedule {
   Schedule sched;
   uint2* d_entries = nullptr;
+  int* d_n3_pairs = nullptr;   // Schedule::n3_pairs / n3_off (level-structured bases)
+  int* d_n3_off = nullptr;
 };
 
 // Arguments of a host-buffer call that a cached CUDA graph replays.  The graph
@@ -181,6 +183,8 @@ DevModel make_model(mtp_handle* h, const DeviceSchedule& ds) {
   md.mono_k = h->d_mk;
   md.dense_k = h->d_dense_k;
   md.dm_pos = h->d_dm_pos;
+  md.n3_pairs = ds.d_n3_pairs;
+  md.n3_off = ds.d_n3_off;
   md.Q = s.Q;
   md.npairs = s.npairs;
   md.tri = s.tri ? 1 : 0;
@@ -220,6 +224,14 @@ int get_schedule(mtp_handle* h, int lanes, int width, DeviceSchedule** out) {
     const auto& ent = ds.sched.entries;
     MTP_CUDA(h, dalloc(&ds.d_entries, ent.size() / 2));
     MTP_CUDA(h, cudaMemcpy(ds.d_entries, ent.data(), ent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if (ds.sched.tri) {
+      const auto& np = ds.sched.n3_pairs;
+      const auto& no = ds.sched.n3_off;
+      MTP_CUDA(h, dalloc(&ds.d_n3_pairs, np.size()));
+      MTP_CUDA(h, cudaMemcpy(ds.d_n3_pairs, np.data(), np.size() * sizeof(int), cudaMemcpyHostToDevice));
+      MTP_CUDA(h, dalloc(&ds.d_n3_off, no.size()));
+      MTP_CUDA(h, cudaMemcpy(ds.d_n3_off, no.data(), no.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
     if (h->d_abc == nullptr) {
       MTP_CUDA(h, dalloc(&h->d_abc, ds.sched.mono_abc.size()));
       MTP_CUDA(h, cudaMemcpy(h->d_abc, ds.sched.mono_abc.data(), ds.sched.mono_abc.size() * sizeof(int),
@@ -265,7 +277,11 @@ int upload_coeffs(mtp_handle* h) {
 void free_handle(mtp_handle* h) {
   if (!h) return;
   auto F = [](void* p) { if (p) cudaFree(p); };
-  for (auto& kv : h->scheds) F(kv.second.d_entries);
+  for (auto& kv : h->scheds) {
+    F(kv.second.d_entries);
+    F(kv.second.d_n3_pairs);
+    F(kv.second.d_n3_off);
+  }
   F(h->d_radial); F(h->d_species); F(h->d_theta); F(h->d_seed_val);
   F(h->d_mapping); F(h->d_seed_idx); F(h->d_zero); F(h->d_abc); F(h->d_mk); F(h->d_dense_k); F(h->d_dm_pos);
   F(h->d_itypes); F(h->d_js); F(h->d_jtypes); F(h->d_counts); F(h->d_rijs);

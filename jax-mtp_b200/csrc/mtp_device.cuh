@@ -67,6 +67,8 @@ struct DevModel {
   int tri;                  // Schedule::tri: step k of a force-phase chain has k / 2 + 1 radial functions,
                             // and the basic moments' adjoints are in chain order (dm_pos)
   const int* dm_pos;        // [M] adjoint position of each moment (Schedule::dm_pos)
+  const int* n3_pairs;      // Schedule::n3_pairs / n3_off (level-structured bases)
+  const int* n3_off;
   int nmu[kMaxDegree + 1];  // radial functions with a basic moment of each degree
   int v_m, v_dm, v_zero, v_one, v_size;
   double scaling, rmin, rmax;
@@ -99,17 +101,26 @@ constexpr int kPrefetch = kStepAlign;
 struct SmemLayout {
   int pws;        // stride of a power row (3 (D+1), rounded up to odd)
   bool dmt_in_v;  // dense table in the moment half of the value space
-  size_t v, rad, u, f, fp, pw, slot, dmt, red, cnt, total;
+  bool n3p_in_v;  // force-phase partial sums in the moment half of the value space
+  size_t v, rad, u, f, fp, pw, slot, dmt, n3p, red, cnt, total;
 };
+
+// Values of the force phase's partial-sum buffer on level-structured bases:
+// (G_x, G_y, G_z, S) of 32 neighbours from each warp.
+__host__ __device__ inline int n3_partials(int threads) { return 4 * threads; }
 
 template <typename T>
 __host__ __device__ inline SmemLayout smem_layout(int v_size, int M, int S, int R, int K, int D, int n_pad,
-                                                  int threads, int A) {
+                                                  int threads, int A, bool tri) {
   SmemLayout L;
   L.pws = 3 * (D + 1);
   if ((L.pws & 1) == 0) L.pws += 1;
   const int Q = (D + 1) * (D + 2) * (D + 3) / 6;
-  L.dmt_in_v = v_size > 0 && Q * R <= M;
+  // level-structured bases need no dense table; their partial sums use the
+  // moment half of the value space (dead after the reverse passes) when it
+  // holds them
+  L.dmt_in_v = tri || (v_size > 0 && Q * R <= M);
+  L.n3p_in_v = tri && v_size > 0 && n3_partials(threads) <= M * A;
   size_t o = 0;
   auto take = [&](size_t bytes) {
     size_t at = (o + 31) & ~size_t(31);
@@ -124,6 +135,7 @@ __host__ __device__ inline SmemLayout smem_layout(int v_size, int M, int S, int 
   L.pw = take(sizeof(T) * L.pws * n_pad * A);
   L.slot = take(sizeof(int) * n_pad * A);
   L.dmt = L.dmt_in_v ? L.v : take(sizeof(T) * R * Q * A);
+  L.n3p = !tri || L.n3p_in_v ? L.v : take(sizeof(T) * n3_partials(threads));
   L.red = take(sizeof(double) * (threads / 32) * A);
   L.cnt = take(sizeof(int) * (threads / 32 + 8));   // per-warp counts, then per-atom totals
   L.total = (o + 31) & ~size_t(31);
@@ -281,16 +293,10 @@ __device__ __forceinline__ void stream_entries_n(const uint2* __restrict__ ent, 
 // are per atom, so two neighbours share every row load and their chains run
 // side by side.  The tpn threads of a neighbour pair take the (a, b)
 // pairs in snake order (sl, 2 tpn-1-sl, 2 tpn+sl, ...) of the pair order
-// (a + b ascending), so their shares differ by one pair at most.
-// kTri (Schedule::tri): the chain's step k = top - c has the radial functions
-// mu <= k / 2 only; the chain is unrolled over k so each step does exactly
-// those multiply-adds (level 24: 581 of a dense table's 1,716 (slot, mu)
-// entries), and dmt is the atom's adjoint region in the value space (element
-// stride AS, the block's atoms), whose basic moments are stored in chain order:
-// a pair of diagonal s = a + b starts floor((D - s + 2)^2 / 4) after the
-// previous pair of its diagonal and step k at floor((k + 1)^2 / 4) within it.
-// Otherwise dmt is the dense table [slot][R] in pair order.
-template <typename T, int R, bool kTwo, bool kTri, int AS>
+// (a + b ascending), so their shares differ by one pair at most.  dmt is the
+// dense table [slot][R] in pair order (bases without the level structure;
+// level-structured ones use n3_transposed).
+template <typename T, int R, bool kTwo>
 __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
                                         int npairs, int D1, const T* __restrict__ fq0, const T* __restrict__ fpq0,
                                         const T* __restrict__ fq1, const T* __restrict__ fpq1, bool two,
@@ -307,33 +313,29 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
   // diagonal s = a + b of the current pair, its first pair index, and the
   // first dense slot of the diagonal (pair order: each pair of diagonal s
   // owns D - s + 1 slots, so slot bases follow without a table lookup)
-  int s = 0, sb = 0, slot_sb = 0, cb_sb = 0;
+  int s = 0, sb = 0, slot_sb = 0;
   for (int k = 0;; ++k) {
     const int i = (k >> 1) * 2 * tpn + ((k & 1) ? 2 * tpn - 1 - sl : sl);
     if (i >= npairs) break;
     while (i >= sb + s + 1) {
       sb += s + 1;
       slot_sb += (s + 1) * (D - s + 1);
-      cb_sb += (s + 1) * (((D - s + 2) * (D - s + 2)) >> 2);
       ++s;
     }
     const int ea = i - sb, eb = s - ea, top = D - s;
-    const T* drow = kTri ? dmt + (cb_sb + ea * (((top + 2) * (top + 2)) >> 2)) * AS
-                         : dmt + (slot_sb + ea * (D - s + 1) + top) * R;
+    const T* drow = dmt + (slot_sb + ea * (D - s + 1) + top) * R;
     T h0 = T(0), hz0 = T(0), hs0 = T(0), h1 = T(0), hz1 = T(0), hs1 = T(0);
-    // one Horner step: table row drow, radial functions mu < nm
-    auto step = [&](const T* row, int nm, int stride) {
+    // one Horner step over the table row
+    auto step = [&](const T* row) {
       T w0 = T(0), wp0 = T(0), w1 = T(0), wp1 = T(0);
 #pragma unroll
       for (int mu = 0; mu < R; ++mu) {
-        if (mu < nm) {
-          const T g = row[mu * stride];
-          w0 = dev_fma(g, f0[mu], w0);
-          wp0 = dev_fma(g, fp0[mu], wp0);
-          if (kTwo) {
-            w1 = dev_fma(g, f1[mu], w1);
-            wp1 = dev_fma(g, fp1[mu], wp1);
-          }
+        const T g = row[mu];
+        w0 = dev_fma(g, f0[mu], w0);
+        wp0 = dev_fma(g, fp0[mu], wp0);
+        if (kTwo) {
+          w1 = dev_fma(g, f1[mu], w1);
+          wp1 = dev_fma(g, fp1[mu], wp1);
         }
       }
       hz0 = dev_fma(hz0, uz0, h0);
@@ -345,16 +347,8 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
         hs1 = dev_fma(hs1, uz1, wp1);
       }
     };
-    if (kTri) {
-#pragma unroll
-      for (int k = 0; k <= kMaxDegree; ++k) {
-        if (k > top) break;
-        step(drow + (((k + 1) * (k + 1)) >> 2) * AS, k / 2 + 1, AS);
-      }
-    } else {
 #pragma unroll 1
-      for (int c = top; c >= 0; --c, drow -= R) step(drow, R, 1);
-    }
+    for (int c = top; c >= 0; --c, drow -= R) step(drow);
     {
       const T xa = pw0[ea], yb = pw0[D1 + eb];
       const T dxa = ea > 0 ? static_cast<T>(ea) * pw0[ea - 1] : T(0);
@@ -375,6 +369,117 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
       Gz[1] = dev_fma(xy, hz1, Gz[1]);
       S[1] = dev_fma(xy, hs1, S[1]);
     }
+  }
+}
+
+// Force phase on level-structured bases.  Lanes take the block's kept
+// neighbours (item j = 32 c + lane over the A atoms' lists in turn), warps
+// take disjoint sets of monomial pairs (Schedule::n3_pairs, at most 32 per
+// warp; each lane holds one pair word and the warp shuffles it out), so all
+// lanes of a warp read the same adjoint row at every step (one shared-memory
+// wavefront per gather; the A atoms' values of a slot are adjacent) and no
+// lane reduces with its neighbours.  Per item and pair: the Horner chain in
+// u_z over steps k = 0 .. top with the radial functions mu <= k / 2, then the
+// powers of u_x and u_y; the warps' partial sums (G, S) meet in P
+// ([4][warps][32]) and warp 0 adds them in warp order (deterministic) and
+// writes the slot gradients.
+template <typename T, int A, int R>
+__device__ __forceinline__ void n3_transposed(const DevModel& md, const DevIO& io, const SmemLayout& L,
+                                              unsigned char* smem, const T* __restrict__ V,
+                                              const int (&nv_a)[A], int base, int tid, int NT, T* __restrict__ P) {
+  const int w = tid >> 5, lane = tid & 31, NW = NT >> 5;
+  const int D1 = md.D + 1, pws = L.pws, n_pad = io.n_pad;
+  const int p0 = __ldg(md.n3_off + w), np = __ldg(md.n3_off + w + 1) - p0;
+  const int myword = lane < np ? __ldg(md.n3_pairs + p0 + lane) : 0;
+  int J = 0;
+#pragma unroll
+  for (int a = 0; a < A; ++a) J += nv_a[a];
+  for (int c0 = 0; c0 < J; c0 += 32) {
+    const int j = c0 + lane;
+    const bool act = j < J;
+    int a = 0, q = act ? j : 0;
+#pragma unroll
+    for (int aa = 0; aa + 1 < A; ++aa)
+      if (a == aa && q >= nv_a[aa]) {
+        q -= nv_a[aa];
+        a = aa + 1;
+      }
+    const T* sF = reinterpret_cast<const T*>(smem + L.f) + (static_cast<size_t>(a) * n_pad + q) * R;
+    const T* sFp = reinterpret_cast<const T*>(smem + L.fp) + (static_cast<size_t>(a) * n_pad + q) * R;
+    const T* sU = reinterpret_cast<const T*>(smem + L.u) + (static_cast<size_t>(a) * n_pad + q) * 4;
+    const T* pw = reinterpret_cast<const T*>(smem + L.pw) + (static_cast<size_t>(a) * n_pad + q) * pws;
+    T f[R], fp[R];
+#pragma unroll
+    for (int mu = 0; mu < R; ++mu) {
+      f[mu] = sF[mu];
+      fp[mu] = sFp[mu];
+    }
+    const T uz = sU[2];
+    const T* dmv = V + static_cast<size_t>(md.v_dm) * A + a;
+    T Gx = T(0), Gy = T(0), Gz = T(0), Ss = T(0);
+    for (int pi = 0; pi < np; ++pi) {
+      const int word = __shfl_sync(0xffffffffu, myword, pi);
+      if (act) {
+        const int ea = word & 15, eb = (word >> 4) & 15, top = (word >> 8) & 15;
+        const T* drow = dmv + static_cast<size_t>(word >> 12) * A;
+        T h = T(0), hz = T(0), hs = T(0);
+#pragma unroll
+        for (int k = 0; k <= kMaxDegree; ++k) {
+          if (k > top) break;
+          const T* row = drow + (((k + 1) * (k + 1)) >> 2) * A;
+          T wv = T(0), wp = T(0);
+#pragma unroll
+          for (int mu = 0; mu < R; ++mu) {
+            if (mu <= k / 2) {
+              const T g = row[mu * A];
+              wv = dev_fma(g, f[mu], wv);
+              wp = dev_fma(g, fp[mu], wp);
+            }
+          }
+          hz = dev_fma(hz, uz, h);
+          h = dev_fma(h, uz, wv);
+          hs = dev_fma(hs, uz, wp);
+        }
+        const T xa = pw[ea], yb = pw[D1 + eb];
+        const T dxa = ea > 0 ? static_cast<T>(ea) * pw[ea - 1] : T(0);
+        const T dyb = eb > 0 ? static_cast<T>(eb) * pw[D1 + eb - 1] : T(0);
+        const T xy = xa * yb;
+        Gx = dev_fma(dxa * yb, h, Gx);
+        Gy = dev_fma(xa * dyb, h, Gy);
+        Gz = dev_fma(xy, hz, Gz);
+        Ss = dev_fma(xy, hs, Ss);
+      }
+    }
+    P[(0 * NW + w) * 32 + lane] = Gx;
+    P[(1 * NW + w) * 32 + lane] = Gy;
+    P[(2 * NW + w) * 32 + lane] = Gz;
+    P[(3 * NW + w) * 32 + lane] = Ss;
+    __syncthreads();
+    if (w == 0 && act) {
+      T gx_ = T(0), gy_ = T(0), gz_ = T(0), s_ = T(0);
+      for (int ww = 0; ww < NW; ++ww) {
+        gx_ += P[(0 * NW + ww) * 32 + lane];
+        gy_ += P[(1 * NW + ww) * 32 + lane];
+        gz_ += P[(2 * NW + ww) * 32 + lane];
+        s_ += P[(3 * NW + ww) * 32 + lane];
+      }
+      const T ux = sU[0], uy = sU[1], d = sU[3];
+      const T ug = ux * gx_ + uy * gy_ + uz * gz_;
+      const T inv_d = T(1) / d;
+      const T gx = ux * s_ + (gx_ - ux * ug) * inv_d;
+      const T gy = uy * s_ + (gy_ - uy * ug) * inv_d;
+      const T gz = uz * s_ + (gz_ - uz * ug) * inv_d;
+      const int atom = base + a;
+      const int slot = reinterpret_cast<const int*>(smem + L.slot)[a * n_pad + q];
+      double* grow = io.pair_grad + (static_cast<size_t>(atom) * io.nbr_stride + slot) * 3;
+      grow[0] = static_cast<double>(gx);
+      grow[1] = static_cast<double>(gy);
+      grow[2] = static_cast<double>(gz);
+      if (!(isfinite(static_cast<double>(gx)) && isfinite(static_cast<double>(gy)) &&
+            isfinite(static_cast<double>(gz))))
+        atomicOr(io.err, kErrNonFinite);
+    }
+    __syncthreads();
   }
 }
 
@@ -434,7 +539,8 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
   extern __shared__ __align__(32) unsigned char smem[];
   const int NT = blockDim.x;
   const int tid = threadIdx.x;
-  const SmemLayout L = smem_layout<T>(kVGlobal ? 0 : md.v_size, md.M, md.S, md.R, md.K, md.D, io.n_pad, NT, A);
+  const SmemLayout L = smem_layout<T>(kVGlobal ? 0 : md.v_size, md.M, md.S, md.R, md.K, md.D, io.n_pad, NT, A,
+                                     md.tri != 0);
   T* V = kVGlobal ? reinterpret_cast<T*>(io.vscratch) + static_cast<size_t>(blockIdx.x) * md.v_size * A
                   : reinterpret_cast<T*>(smem + L.v);
   T* sRad = reinterpret_cast<T*>(smem + L.rad);
@@ -702,16 +808,27 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
     // order); otherwise a dense table Dm[a][slot][mu] = dE/dm of basic moment
     // (mu, slot) over the full monomial simplex in pair order (0 where the
     // basis has no moment) is filled first
-    T* sDm = L.dmt_in_v ? V + md.v_m * A : reinterpret_cast<T*>(smem + L.dmt);
-    const int QR = md.Q * R;
-    if (!md.tri) {
-      for (int x = tid; x < QR * A; x += NT) {
-        const int a = x / QR, r = x - a * QR;
-        const int k = __ldg(md.dense_k + (r / R) * kMaxR + r % R);
-        sDm[x] = k >= 0 ? V[(md.v_dm + __ldg(md.dm_pos + k)) * A + a] : T(0);
+    if (md.tri) {
+      T* P = L.n3p_in_v ? V + static_cast<size_t>(md.v_m) * A : reinterpret_cast<T*>(smem + L.n3p);
+      switch (R) {
+#define MTP_N3T_CASE(RR) \
+  case RR: n3_transposed<T, A, RR>(md, io, L, smem, V, nv_a, base, tid, NT, P); break;
+        MTP_N3T_CASE(1) MTP_N3T_CASE(2) MTP_N3T_CASE(3) MTP_N3T_CASE(4)
+        MTP_N3T_CASE(5) MTP_N3T_CASE(6) MTP_N3T_CASE(7) MTP_N3T_CASE(8)
+#undef MTP_N3T_CASE
+        default: break;
       }
       __syncthreads();
+      continue;
     }
+    T* sDm = L.dmt_in_v ? V + md.v_m * A : reinterpret_cast<T*>(smem + L.dmt);
+    const int QR = md.Q * R;
+    for (int x = tid; x < QR * A; x += NT) {
+      const int a = x / QR, r = x - a * QR;
+      const int k = __ldg(md.dense_k + (r / R) * kMaxR + r % R);
+      sDm[x] = k >= 0 ? V[(md.v_dm + __ldg(md.dm_pos + k)) * A + a] : T(0);
+    }
+    __syncthreads();
 #pragma unroll
     for (int a = 0; a < A; ++a) {
       const int atom = base + a;
@@ -739,17 +856,12 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
         const int sl = idx & (tpn - 1);
         T Ssum[2] = {T(0), T(0)}, Gx[2] = {T(0), T(0)}, Gy[2] = {T(0), T(0)}, Gz[2] = {T(0), T(0)};
         if (active) {
-          const T* dmt = md.tri ? V + static_cast<size_t>(md.v_dm) * A + a : sDm + static_cast<size_t>(a) * QR;
+          const T* dmt = sDm + static_cast<size_t>(a) * QR;
           const int qb = two ? q1 : q0;
           switch (R) {
 #define MTP_N3_CASE(RR)                                                                                        \
   case RR:                                                                                                     \
-    if (md.tri)                                                                                                \
-      n3_sums<T, RR, kTwoN, true, A>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R,          \
-                                  sFp + qb * R, two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2],          \
-                                  sU[4 * qb + 2], sl, tpn, Ssum, Gx, Gy, Gz);                                 \
-    else                                                                                                       \
-      n3_sums<T, RR, kTwoN, false, 1>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R,         \
+    n3_sums<T, RR, kTwoN>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R,         \
                                    sFp + qb * R, two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2],         \
                                    sU[4 * qb + 2], sl, tpn, Ssum, Gx, Gy, Gz);                                \
     break;

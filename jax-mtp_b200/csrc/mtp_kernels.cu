@@ -13,8 +13,8 @@ namespace mtp {
 // ---------------------------------------------------------------------------
 size_t eval_smem_bytes(const DevModel& md, int n_pad, int threads, bool fp64, bool vglobal, int A) {
   const int vs = vglobal ? 0 : md.v_size;
-  SmemLayout L = fp64 ? smem_layout<double>(vs, md.M, md.S, md.R, md.K, md.D, n_pad, threads, A)
-                      : smem_layout<float>(vs, md.M, md.S, md.R, md.K, md.D, n_pad, threads, A);
+  SmemLayout L = fp64 ? smem_layout<double>(vs, md.M, md.S, md.R, md.K, md.D, n_pad, threads, A, md.tri != 0)
+                      : smem_layout<float>(vs, md.M, md.S, md.R, md.K, md.D, n_pad, threads, A, md.tri != 0);
   return L.total;
 }
 

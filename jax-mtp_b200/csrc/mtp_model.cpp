@@ -546,6 +546,42 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
     }
   }
   s.tri = adjoint_layout(pot, s.dm_pos);
+  if (s.tri) {
+    // pairs (a, b) in pair order with their chain base; longest chain first
+    // onto the least loaded warp (cost ~ adjoint loads and multiply-adds of the
+    // chain's steps plus its Horner steps and tail)
+    struct P3 { int word, cost; };
+    std::vector<P3> pairs;
+    int base = 0;
+    for (int sum = 0; sum <= s.D; ++sum)
+      for (int a = 0; a <= sum; ++a) {
+        const int b = sum - a, top = s.D - sum;
+        int cost = 10;
+        for (int k = 0; k <= top; ++k) cost += 3 * (k / 2 + 1) + 3;
+        pairs.push_back({a | (b << 4) | (top << 8) | (base << 12), cost});
+        base += ((top + 2) * (top + 2)) / 4;
+      }
+    const int warps = lanes / 32;
+    std::vector<int> order(pairs.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return pairs[x].cost > pairs[y].cost; });
+    std::vector<std::vector<int>> wl(warps);
+    std::vector<long> load(warps, 0);
+    for (int i : order) {
+      int w = 0;
+      for (int v = 1; v < warps; ++v)
+        if (load[v] < load[w] || (load[v] == load[w] && wl[v].size() < wl[w].size())) w = v;
+      wl[w].push_back(pairs[i].word);
+      load[w] += pairs[i].cost;
+    }
+    s.n3_off.assign(1, 0);
+    for (int w = 0; w < warps; ++w) {
+      if (wl[w].size() > 32) s.tri = false;    // one pair per lane at most
+      s.n3_pairs.insert(s.n3_pairs.end(), wl[w].begin(), wl[w].end());
+      s.n3_off.push_back(static_cast<int>(s.n3_pairs.size()));
+    }
+    if (base >= (1 << 20) || s.D > 15) s.tri = false;
+  }
   // moments that are read but never written stay zero for the whole run
   std::vector<char> read(M, 0);
   for (int e = 0; e < T; ++e) { read[pot.times[4 * e]] = 1; read[pot.times[4 * e + 1]] = 1; }

@@ -96,6 +96,11 @@ struct Schedule {
   bool tri = false;
   // dE/dm of moment k lives at v_dm + dm_pos[k] (a permutation of [0, M))
   std::vector<int> dm_pos;
+  // Force phase on level-structured bases: warp w of the block takes the
+  // monomial pairs n3_pairs[n3_off[w] .. n3_off[w + 1]) (at most 32, balanced
+  // by chain cost), each one word a | b << 4 | top << 8 | chain base << 12
+  // (top = D - a - b; chain base = the pair's first adjoint position).
+  std::vector<int> n3_pairs, n3_off;
   std::vector<int> zero_list;   // non-basic moments never written (must read as 0)
   std::vector<Pass> fwd, rev;   // passes in execution order
   std::vector<uint32_t> entries;  // pairs (x, y) per entry: 2 words; kStepAlign no-op rows at the end

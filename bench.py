@@ -360,6 +360,8 @@ def run_ours(args):
     ran = tuning["mixed"]["ran"]
     traffic_rec = read_traffic(ran["threads"], ran["atoms_per_block"])
     traffic = traffic_rec["bytes_per_launch"] if traffic_rec else None
+    ran64 = tuning["fp64"]["ran"]
+    traffic64_rec = read_traffic(ran64["threads"], ran64["atoms_per_block"], "fp64")
     # the same launch against HBM: algorithmic bytes per atom-step through the
     # evaluation (28 n_pad + 36: r_ij and neighbour index in, force and energy out)
     alg_bytes = (28 * STRIDE + 36) * N
@@ -380,6 +382,13 @@ def run_ours(args):
     if rank == 0 and not args.skip_e2e:
         e2e = run_e2e(eng["mixed"], mds["mixed"], N, args)
 
+    # the LAMMPS-size legs run with the 1M-atom engines and their pinned
+    # buffers released (with them alive the small calls ran up to 1.9x slower)
+    for p in ("mixed", "fp64"):
+        eng[p].close()
+    del mds
+    torch.cuda.empty_cache()
+
     pair_call = None
     if rank == 0 and not args.skip_e2e:
         pair_call = run_pair_call(args)
@@ -391,11 +400,6 @@ def run_ours(args):
     pair_nve = None
     if rank == 0 and world == 1 and not args.skip_e2e and args.pair_nve_steps > 0:
         pair_nve = run_pair_style_nve(args.pair_nve_steps)
-
-    for p in ("mixed", "fp64"):
-        eng[p].close()
-    del mds
-    torch.cuda.empty_cache()
     train = None
     if not args.skip_train:
         train = run_train(args, device, dist)
@@ -421,7 +425,8 @@ def run_ours(args):
                          "peak_source": "measured live: FP32 FMA-chain kernel (no FP32/FP64 CUDA-core peak in "
                                         "MEASURED_PEAKS.json)",
                          "fp64_kernel": {"achieved": achieved64, "peak": fp64_peak, "frac": achieved64 / fp64_peak
-                                         if fp64_peak else None, "kernel_ms": k_64 * 1e3}},
+                                         if fp64_peak else None, "kernel_ms": k_64 * 1e3,
+                                         "traffic": traffic64_rec["bytes_per_launch"] if traffic64_rec else None}},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "pair_style_call": pair_call,
@@ -847,12 +852,15 @@ def run_pair_call(args):
                              ("mtp_execute_potential", bridge), ("mtp_compute_positions", positions)):
                 for _ in range(5):
                     fn()
+                st0 = eng.stats()
                 t0 = time.perf_counter()
                 for _ in range(calls):
                     fn()
                 us = (time.perf_counter() - t0) / calls * 1e6
+                st1 = eng.stats()
                 out[f"{prec}_{name}_us"] = us
                 out[f"{prec}_{name}_atom_steps_per_s"] = N / (us * 1e-6)
+                out[f"{prec}_{name}_graph_replays"] = int(st1["graph_replays"] - st0["graph_replays"])
     return out
 
 

@@ -36,8 +36,9 @@ def write_traffic(json_path: str, csv_path: str, key: str, kernel: str, scale: f
     the JSON data file under `key`."""
     import csv
     rows = list(csv.reader(open(csv_path)))
-    head = rows[0]
-    units = rows[1]
+    # the header row names the columns (lines the profiled program printed may precede it)
+    at = next(i for i, r in enumerate(rows) if "Kernel Name" in r)
+    head, units, rows = rows[at], rows[at + 1], rows[at:]
     iname = head.index("Kernel Name")
     irx, iwx = head.index("dram__bytes_read.sum"), head.index("dram__bytes_write.sum")
     per = []

@@ -35,6 +35,7 @@ struct DeviceSchedule {
   uint2* d_entries = nullptr;
   int* d_n3_pairs = nullptr;   // Schedule::n3_pairs / n3_off (level-structured bases)
   int* d_n3_off = nullptr;
+  int* d_warp_steps = nullptr;  // [forward passes, reverse passes][lanes / 32] (Pass::wsteps)
 };
 
 // Arguments of a host-buffer call that a cached CUDA graph replays.  The graph
@@ -185,6 +186,7 @@ DevModel make_model(mtp_handle* h, const DeviceSchedule& ds) {
   md.dm_pos = h->d_dm_pos;
   md.n3_pairs = ds.d_n3_pairs;
   md.n3_off = ds.d_n3_off;
+  md.warp_steps = ds.d_warp_steps;
   md.Q = s.Q;
   md.npairs = s.npairs;
   md.tri = s.tri ? 1 : 0;
@@ -224,6 +226,13 @@ int get_schedule(mtp_handle* h, int lanes, int width, DeviceSchedule** out) {
     const auto& ent = ds.sched.entries;
     MTP_CUDA(h, dalloc(&ds.d_entries, ent.size() / 2));
     MTP_CUDA(h, cudaMemcpy(ds.d_entries, ent.data(), ent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    {
+      std::vector<int> ws;
+      for (const Pass& p : ds.sched.fwd) ws.insert(ws.end(), p.wsteps.begin(), p.wsteps.end());
+      for (const Pass& p : ds.sched.rev) ws.insert(ws.end(), p.wsteps.begin(), p.wsteps.end());
+      MTP_CUDA(h, dalloc(&ds.d_warp_steps, ws.size()));
+      MTP_CUDA(h, cudaMemcpy(ds.d_warp_steps, ws.data(), ws.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
     if (ds.sched.tri) {
       const auto& np = ds.sched.n3_pairs;
       const auto& no = ds.sched.n3_off;
@@ -281,6 +290,7 @@ void free_handle(mtp_handle* h) {
     F(kv.second.d_entries);
     F(kv.second.d_n3_pairs);
     F(kv.second.d_n3_off);
+    F(kv.second.d_warp_steps);
   }
   F(h->d_radial); F(h->d_species); F(h->d_theta); F(h->d_seed_val);
   F(h->d_mapping); F(h->d_seed_idx); F(h->d_zero); F(h->d_abc); F(h->d_mk); F(h->d_dense_k); F(h->d_dm_pos);

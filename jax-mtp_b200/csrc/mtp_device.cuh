@@ -51,6 +51,9 @@ struct DevModel {
   DevPass fwd[kMaxPasses];
   DevPass rev[kMaxPasses];
   int nfwd, nrev;
+  // steps each warp runs in each pass, [nfwd + nrev][lanes / 32]: a warp
+  // stops after its longest lane's program (Pass::wsteps)
+  const int* warp_steps;
   const double* radial;     // [S][S][R][K]
   const double* species;    // [S]
   const double* theta;      // [Sa]
@@ -232,6 +235,14 @@ __device__ __forceinline__ void run_pass(const uint2* __restrict__ ent, int step
       }
     }
   }
+}
+
+// Lane p of every warp gets its warp's step count of pass p (forward passes,
+// then reverse ones; at most 32 passes), so a pass reads its count with a
+// shuffle instead of a load.
+__device__ __forceinline__ int warp_steps_of_lane(const DevModel& md, int tid, int NT) {
+  const int p = tid & 31;
+  return p < md.nfwd + md.nrev ? __ldg(md.warp_steps + p * (NT >> 5) + (tid >> 5)) : 0;
 }
 
 // run_pass for the block's lane count (128, 256 or 512 threads).
@@ -539,6 +550,9 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
   extern __shared__ __align__(32) unsigned char smem[];
   const int NT = blockDim.x;
   const int tid = threadIdx.x;
+  // this warp's step count of pass p (forward passes, then reverse ones) is
+  // held by lane p and shuffled out at the pass: no load before a pass
+  const int my_wsteps = warp_steps_of_lane(md, tid, NT);
   const SmemLayout L = smem_layout<T>(kVGlobal ? 0 : md.v_size, md.M, md.S, md.R, md.K, md.D, io.n_pad, NT, A,
                                      md.tri != 0);
   T* V = kVGlobal ? reinterpret_cast<T*>(io.vscratch) + static_cast<size_t>(blockIdx.x) * md.v_size * A
@@ -562,6 +576,21 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
   __syncthreads();
 
   for (int base = blockIdx.x * A; base < io.natoms; base += gridDim.x * A) {
+    // ask L2 for the rows of this block's next atoms now, so their staging
+    // loads find them there instead of in DRAM (a hint; nothing waits on it)
+    {
+      const int next = base + gridDim.x * A;
+      if (next < io.natoms) {
+        const int na = min(A, io.natoms - next);
+        const char* r0 = reinterpret_cast<const char*>(io.rijs + static_cast<size_t>(next) * io.nbr_stride * 3);
+        const char* t0 = reinterpret_cast<const char*>(io.jtypes + static_cast<size_t>(next) * io.nbr_stride);
+        const int rl = (na * io.nbr_stride * 24 + 127) >> 7, tl = (na * io.nbr_stride * 4 + 127) >> 7;
+        for (int x = tid; x < rl + tl; x += NT) {
+          const char* a = x < rl ? r0 + 128 * static_cast<size_t>(x) : t0 + 128 * static_cast<size_t>(x - rl);
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+        }
+      }
+    }
     // moments that are read but never written (the force phase of the
     // previous atom may have reused their slots for its dense table)
     for (int x = tid; x < md.nzero * A; x += NT) V[(md.v_m + md.zero_list[x / A]) * A + x % A] = T(0);
@@ -770,7 +799,8 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
 
     // ---- T: forward contraction passes ----------------------------------
     for (int ps = 0; ps < md.nfwd; ++ps) {
-      run_pass_n<T, A, kVGlobal>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, V);
+      run_pass_n<T, A, kVGlobal>(md.entries + md.fwd[ps].offset, __shfl_sync(0xFFFFFFFFu, my_wsteps, ps), NT, tid,
+                                 V);
       __syncthreads();
     }
     // energy: E_i = xi[t_i] + sum_alpha theta_alpha m[map_alpha] in FP64
@@ -799,7 +829,8 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
 
     // ---- R: reverse passes (dE/dm) ---------------------------------------
     for (int ps = 0; ps < md.nrev; ++ps) {
-      run_pass_n<T, A, kVGlobal>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, V);
+      run_pass_n<T, A, kVGlobal>(md.entries + md.rev[ps].offset,
+                                 __shfl_sync(0xFFFFFFFFu, my_wsteps, md.nfwd + ps), NT, tid, V);
       __syncthreads();
     }
 

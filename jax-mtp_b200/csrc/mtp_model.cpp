@@ -251,7 +251,8 @@ struct RawEntry {
 };
 struct RawPass {
   int steps = 0;
-  std::vector<RawEntry> e;  // [steps][lanes]
+  std::vector<RawEntry> e;    // [steps][lanes]
+  std::vector<int> lane_len;  // real entries of each lane (the rest of its column is padding)
 };
 
 // Lay jobs onto lanes (longest first onto the least loaded lane), then order
@@ -282,12 +283,24 @@ RawPass lay_out(const std::vector<Job>& jobs, int lanes, int width, bool allow_s
     lane_jobs[top.second].push_back(j);
     heap.push({top.first + jobs[j].sides.size(), top.second});
   }
+  // longest lanes first, so the short ones share warps that stop early
+  // (every warp runs only its own longest lane's steps)
+  auto lane_total = [&](const std::vector<int>& js) {
+    size_t n = 0;
+    for (int j : js) n += jobs[j].sides.size();
+    return n;
+  };
+  std::stable_sort(lane_jobs.begin(), lane_jobs.end(), [&](const std::vector<int>& x, const std::vector<int>& y) {
+    return lane_total(x) > lane_total(y);
+  });
   RawPass p;
   size_t steps = 0;
+  p.lane_len.assign(lanes, 0);
   for (int l = 0; l < lanes; ++l) {
     size_t n = 0;
     for (int j : lane_jobs[l]) n += jobs[j].sides.size();
     steps = std::max(steps, n);
+    p.lane_len[l] = static_cast<int>(n);
   }
   p.steps = static_cast<int>(steps);
   p.e.assign(steps * lanes, RawEntry{kSymZero, kSymZero, kSymZero, kOpNone, 0});
@@ -670,6 +683,9 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
       Pass p;
       p.offset = static_cast<int>(s.entries.size() / 2);
       p.steps = (rp.steps + kStepAlign - 1) / kStepAlign * kStepAlign;
+      p.wsteps.assign(lanes / 32, 0);
+      for (int l = 0; l < lanes; ++l)
+        p.wsteps[l / 32] = std::max(p.wsteps[l / 32], (rp.lane_len[l] + kStepAlign - 1) / kStepAlign * kStepAlign);
       for (const RawEntry& r : rp.e) {
         uint32_t a = resolve(r.a), b = resolve(r.b), d = resolve(r.dst);
         s.entries.push_back(a | (b << 16));
@@ -710,7 +726,8 @@ double emulate_schedule(const Potential& pot, const Schedule& s, std::vector<dou
     std::vector<std::pair<int, std::pair<int, double>>> writes;
     for (int l = 0; l < s.lanes; ++l) {
       double acc = 0.0;
-      for (int st = 0; st < p.steps; ++st) {
+      // a warp runs only its own step count (Pass::wsteps), as on the device
+      for (int st = 0; st < p.wsteps[l / 32]; ++st) {
         size_t e = static_cast<size_t>(p.offset) + static_cast<size_t>(st) * s.lanes + l;
         uint32_t x = s.entries[2 * e], y = s.entries[2 * e + 1];
         int a = x & 0xFFFF, b = x >> 16, d = y >> kDstShift, op = (y >> kOpShift) & 3;

@@ -63,6 +63,9 @@ constexpr int kDstShift = 16;
 struct Pass {
   int offset = 0;   // first entry (index into Schedule::entries)
   int steps = 0;    // entries per lane (a multiple of kStepAlign)
+  // steps each warp of the block runs: its longest lane's program rounded up
+  // to kStepAlign (the rows after that are no-ops for all of its lanes)
+  std::vector<int> wsteps;
 };
 
 struct Schedule {

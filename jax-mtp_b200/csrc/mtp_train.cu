@@ -126,6 +126,7 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
                                                      double* partials) {
   extern __shared__ __align__(32) unsigned char smem[];
   const int NT = blockDim.x, tid = threadIdx.x;
+  const int my_wsteps = warp_steps_of_lane(md, tid, NT);
   const int S = md.S, R = md.R, K = md.K, P = md.P, D1 = md.D + 1;
   const TrainSmem L = train_layout<T>(kVGlobal ? 0 : md.v_size, S, R, K, P, md.D, md.Sa, n_pad, NT);
   using T2 = typename Dual2<T>::type;
@@ -365,7 +366,8 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
     // ---- dual forward tree --------------------------------------------------
     for (int ps = 0; ps < md.nfwd; ++ps) {
       DualFwdBody<T> body{V, V, T(0), T(0)};
-      stream_entries_n<kStreamDepth, kVGlobal>(md.entries + md.fwd[ps].offset, md.fwd[ps].steps, NT, tid, body);
+      stream_entries_n<kStreamDepth, kVGlobal>(md.entries + md.fwd[ps].offset,
+                                               __shfl_sync(0xFFFFFFFFu, my_wsteps, ps), NT, tid, body);
       __syncthreads();
     }
     for (int a = tid; a < md.Sa; a += NT) {
@@ -377,7 +379,8 @@ __global__ void __launch_bounds__(512) k_mtp_adjoint(DevModel md, TrainIO io, in
     // ---- dual reverse tree ---------------------------------------------------
     for (int ps = 0; ps < md.nrev; ++ps) {
       DualRevBody<T> body{V, V, T(0), T(0)};
-      stream_entries_n<kStreamDepth, kVGlobal>(md.entries + md.rev[ps].offset, md.rev[ps].steps, NT, tid, body);
+      stream_entries_n<kStreamDepth, kVGlobal>(md.entries + md.rev[ps].offset,
+                                               __shfl_sync(0xFFFFFFFFu, my_wsteps, md.nfwd + ps), NT, tid, body);
       __syncthreads();
     }
 

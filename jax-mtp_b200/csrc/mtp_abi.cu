@@ -214,33 +214,22 @@ DevModel make_model(mtp_handle* h, const DeviceSchedule& ds) {
 // the schedule's entry order is tuned for).
 inline int access_width(bool fp64, int atoms_per_block) { return (fp64 ? 8 : 4) * atoms_per_block; }
 
-// Schedule for `lanes` threads and `width`-byte operand accesses, built and
-// uploaded on first use.
-int get_schedule(mtp_handle* h, int lanes, int width, DeviceSchedule** out) {
+// Dynamic shared memory one block of this part can opt in to.
+constexpr size_t kMaxSmemPerBlock = 227 * 1024;
+
+// Schedule for `lanes` threads and `width`-byte operand accesses, built on
+// first use.  With `upload` (every call that launches with it) its programs
+// also go to the device on first use, after refine_schedule where the value
+// space can sit in shared memory (bank order matters only there); a schedule
+// that is only sized (launch-shape candidates) is neither refined nor
+// uploaded, and no launch ever sees an unrefined copy of a refined one.
+int get_schedule(mtp_handle* h, int lanes, int width, DeviceSchedule** out, bool upload = true) {
   const int key = lanes * 64 + width;
   auto it = h->scheds.find(key);
   if (it == h->scheds.end()) {
     DeviceSchedule ds;
     std::string err;
     if (!build_schedule(h->pot, lanes, ds.sched, err, width)) return fail(h, MTP_E_FORMAT, err);
-    const auto& ent = ds.sched.entries;
-    MTP_CUDA(h, dalloc(&ds.d_entries, ent.size() / 2));
-    MTP_CUDA(h, cudaMemcpy(ds.d_entries, ent.data(), ent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    {
-      std::vector<int> ws;
-      for (const Pass& p : ds.sched.fwd) ws.insert(ws.end(), p.wsteps.begin(), p.wsteps.end());
-      for (const Pass& p : ds.sched.rev) ws.insert(ws.end(), p.wsteps.begin(), p.wsteps.end());
-      MTP_CUDA(h, dalloc(&ds.d_warp_steps, ws.size()));
-      MTP_CUDA(h, cudaMemcpy(ds.d_warp_steps, ws.data(), ws.size() * sizeof(int), cudaMemcpyHostToDevice));
-    }
-    if (ds.sched.tri) {
-      const auto& np = ds.sched.n3_pairs;
-      const auto& no = ds.sched.n3_off;
-      MTP_CUDA(h, dalloc(&ds.d_n3_pairs, np.size()));
-      MTP_CUDA(h, cudaMemcpy(ds.d_n3_pairs, np.data(), np.size() * sizeof(int), cudaMemcpyHostToDevice));
-      MTP_CUDA(h, dalloc(&ds.d_n3_off, no.size()));
-      MTP_CUDA(h, cudaMemcpy(ds.d_n3_off, no.data(), no.size() * sizeof(int), cudaMemcpyHostToDevice));
-    }
     if (h->d_abc == nullptr) {
       MTP_CUDA(h, dalloc(&h->d_abc, ds.sched.mono_abc.size()));
       MTP_CUDA(h, cudaMemcpy(h->d_abc, ds.sched.mono_abc.data(), ds.sched.mono_abc.size() * sizeof(int),
@@ -261,7 +250,27 @@ int get_schedule(mtp_handle* h, int lanes, int width, DeviceSchedule** out) {
     }
     it = h->scheds.emplace(key, ds).first;
   }
-  *out = &it->second;
+  DeviceSchedule& ds = it->second;
+  if (upload && ds.d_entries == nullptr) {
+    if (static_cast<size_t>(ds.sched.v_size) * width <= kMaxSmemPerBlock) refine_schedule(ds.sched);
+    const auto& ent = ds.sched.entries;
+    MTP_CUDA(h, dalloc(&ds.d_entries, ent.size() / 2));
+    MTP_CUDA(h, cudaMemcpy(ds.d_entries, ent.data(), ent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    std::vector<int> ws;
+    for (const Pass& p : ds.sched.fwd) ws.insert(ws.end(), p.wsteps.begin(), p.wsteps.end());
+    for (const Pass& p : ds.sched.rev) ws.insert(ws.end(), p.wsteps.begin(), p.wsteps.end());
+    MTP_CUDA(h, dalloc(&ds.d_warp_steps, ws.size()));
+    MTP_CUDA(h, cudaMemcpy(ds.d_warp_steps, ws.data(), ws.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (ds.sched.tri) {
+      const auto& np = ds.sched.n3_pairs;
+      const auto& no = ds.sched.n3_off;
+      MTP_CUDA(h, dalloc(&ds.d_n3_pairs, np.size()));
+      MTP_CUDA(h, cudaMemcpy(ds.d_n3_pairs, np.data(), np.size() * sizeof(int), cudaMemcpyHostToDevice));
+      MTP_CUDA(h, dalloc(&ds.d_n3_off, no.size()));
+      MTP_CUDA(h, cudaMemcpy(ds.d_n3_off, no.data(), no.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+  }
+  *out = &ds;
   return MTP_OK;
 }
 
@@ -345,7 +354,7 @@ int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, 
       for (int A : a_c) {
         if (!eval_variant_exists(fp64, false, A)) continue;
         DeviceSchedule* ds = nullptr;
-        int st = get_schedule(h, lanes, access_width(fp64, A), &ds);
+        int st = get_schedule(h, lanes, access_width(fp64, A), &ds, false);
         if (st != MTP_OK) return st;
         const DevModel md = make_model(h, *ds);
         int bps = eval_blocks_per_sm(md, stride, lanes, fp64, false, A);
@@ -363,7 +372,7 @@ int pick_launch(mtp_handle* h, int natoms, int stride, DeviceSchedule** ds_out, 
       // block, so the blocks' value spaces stay within L2
       const int lanes = 512;
       DeviceSchedule* ds = nullptr;
-      int st = get_schedule(h, lanes, access_width(fp64, 1), &ds);
+      int st = get_schedule(h, lanes, access_width(fp64, 1), &ds, false);
       if (st != MTP_OK) return st;
       int bps = eval_blocks_per_sm(make_model(h, *ds), stride, lanes, fp64, true, 1);
       if (h->blocks_per_sm > 0) bps = std::min(bps, h->blocks_per_sm);
@@ -707,6 +716,7 @@ int mtp_schedule_emulate(const char* path, int lanes, int width, const double* b
   if (!parse_mtp_file(path, pot, err)) return MTP_E_FORMAT;
   Schedule s;
   if (!build_schedule(pot, lanes, s, err, width)) return MTP_E_FORMAT;
+  refine_schedule(s);
   std::vector<double> V(s.v_size, 0.0);
   for (int k = 0; k < pot.B; ++k) V[s.v_m + k] = basic[k];
   double e = emulate_schedule(pot, s, V);
@@ -792,7 +802,7 @@ int mtp_create(const char* mtp_path, int max_atoms, int max_nbr, double cutoff, 
   int st = upload_coeffs(h);
   if (st != MTP_OK) return bail(st);
   DeviceSchedule* ds = nullptr;
-  st = get_schedule(h, h->threads, access_width(precision == MTP_PRECISION_FP64, 1), &ds);
+  st = get_schedule(h, h->threads, access_width(precision == MTP_PRECISION_FP64, 1), &ds, false);
   if (st != MTP_OK) return bail(st);
   if (h->debug >= 1) {
     std::fprintf(stderr, "[mtp_b200] %s: S=%d R=%d K=%d M=%d B=%d T=%d Sa=%d; %d fwd + %d rev passes, %d value slots\n",
@@ -1214,13 +1224,11 @@ int mtp_adjoint_batch_device(mtp_handle* h, int natoms, int stride, int nconfig,
   // warps for the same L2 footprint
   int lanes = h->threads;
   DeviceSchedule* ds = nullptr;
-  int st = get_schedule(h, lanes, access_width(true, 1), &ds);
+  int st = get_schedule(h, lanes, access_width(true, 1), &ds, false);
   if (st != MTP_OK) return st;
-  if (lanes < 512 && !adjoint_fits_shared(make_model(h, *ds), stride, lanes)) {
-    lanes = 512;
-    st = get_schedule(h, lanes, access_width(true, 1), &ds);
-    if (st != MTP_OK) return st;
-  }
+  if (lanes < 512 && !adjoint_fits_shared(make_model(h, *ds), stride, lanes)) lanes = 512;
+  st = get_schedule(h, lanes, access_width(true, 1), &ds);
+  if (st != MTP_OK) return st;
   DevModel md = make_model(h, *ds);
   TrainIO tio{};
   tio.natoms = natoms;

@@ -714,6 +714,136 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
   return true;
 }
 
+namespace {
+
+// Shared-memory wavefronts of one operand gather (x = the a or b field) of the
+// lanes [g0, g0 + n) at one step of a pass: the most distinct addresses one
+// bank key receives.  The constant slots (zero, one) are read by many lanes at
+// once (broadcasts) and count as free.  `hot` gets the lanes whose key has
+// that many: only moving one of them can lower the count.
+uint32_t gather_wavefronts(const uint32_t* ent, int lanes, size_t row, int g0, int n, bool b_field, uint32_t nkey,
+                           uint32_t free0, uint32_t free1, uint32_t* hot) {
+  uint32_t addr[32], key_n[32] = {};
+  int na = 0;
+  for (int i = 0; i < n; ++i) {
+    const uint32_t w = ent[2 * (row * lanes + g0 + i)];
+    const uint32_t x = b_field ? w >> 16 : w & 0xFFFFu;
+    if (x == free0 || x == free1) continue;
+    bool seen = false;
+    for (int k = 0; k < na && !seen; ++k) seen = addr[k] == x;
+    if (!seen) {
+      addr[na++] = x;
+      ++key_n[x % nkey];
+    }
+  }
+  uint32_t mx = 0;
+  for (uint32_t k = 0; k < nkey; ++k) mx = std::max(mx, key_n[k]);
+  if (hot) {
+    *hot = 0;
+    if (mx > 1)
+      for (int i = 0; i < n; ++i) {
+        const uint32_t w = ent[2 * (row * lanes + g0 + i)];
+        const uint32_t x = b_field ? w >> 16 : w & 0xFFFFu;
+        if (x != free0 && x != free1 && key_n[x % nkey] == mx) *hot |= 1u << i;
+      }
+  }
+  return mx;
+}
+
+}  // namespace
+
+void refine_schedule(Schedule& s) {
+  const int lanes = s.lanes;
+  const int group = std::max(1, std::min(32, 128 / std::max(4, s.width)));
+  const uint32_t nkey = static_cast<uint32_t>(group);
+  const uint32_t z = static_cast<uint32_t>(s.v_zero), one = static_cast<uint32_t>(s.v_one);
+  constexpr int kTries = 16, kSweeps = 2;
+  uint32_t* ent = s.entries.data();
+  uint64_t rng = 0x9E3779B97F4A7C15ull;
+  auto next = [&]() {
+    rng ^= rng << 13;
+    rng ^= rng >> 7;
+    rng ^= rng << 17;
+    return rng;
+  };
+  auto refine_pass = [&](const Pass& p, bool allow_swap) {
+    const size_t steps = static_cast<size_t>(p.steps);
+    uint32_t* e = ent + 2 * static_cast<size_t>(p.offset);
+    // job spans: a lane's job ends at the entry that flushes; entries after
+    // the lane's last flush are padding
+    std::vector<int> lo(steps * lanes, 0), hi(steps * lanes, 0);
+    for (int l = 0; l < lanes; ++l) {
+      size_t start = 0;
+      for (size_t t = 0; t < steps; ++t) {
+        if (((e[2 * (t * lanes + l) + 1] >> kOpShift) & 3u) == kOpNone) continue;
+        for (size_t u = start; u <= t; ++u) {
+          lo[u * lanes + l] = static_cast<int>(start);
+          hi[u * lanes + l] = static_cast<int>(t + 1);
+        }
+        start = t + 1;
+      }
+    }
+    auto cost = [&](size_t t, int g0, int n) {
+      return gather_wavefronts(e, lanes, t, g0, n, false, nkey, z, one, nullptr) +
+             gather_wavefronts(e, lanes, t, g0, n, true, nkey, z, one, nullptr);
+    };
+    // trade the operands and multiplicity of two entries (flush bits stay)
+    auto trade = [&](size_t x, size_t y) {
+      std::swap(e[2 * x], e[2 * y]);
+      const uint32_t mx = e[2 * x + 1] & kMultMask, my = e[2 * y + 1] & kMultMask;
+      e[2 * x + 1] = (e[2 * x + 1] & ~kMultMask) | my;
+      e[2 * y + 1] = (e[2 * y + 1] & ~kMultMask) | mx;
+    };
+    auto flip = [&](size_t x) { e[2 * x] = (e[2 * x] >> 16) | (e[2 * x] << 16); };
+    for (int sweep = 0; sweep < kSweeps; ++sweep) {
+      size_t gained = 0;
+      for (size_t t = 0; t < steps; ++t) {
+        for (int g0 = 0; g0 < lanes; g0 += group) {
+          const int n = std::min(group, lanes - g0);
+          uint32_t hotA, hotB;
+          size_t c0 = gather_wavefronts(e, lanes, t, g0, n, false, nkey, z, one, &hotA) +
+                      gather_wavefronts(e, lanes, t, g0, n, true, nkey, z, one, &hotB);
+          const uint32_t hot = hotA | hotB;
+          for (int i = 0; i < n && c0 > 2; ++i) {
+            if (!(hot >> i & 1u)) continue;
+            const size_t at = t * lanes + g0 + i;
+            if (hi[at] == 0) continue;   // padding
+            if (allow_swap) {
+              flip(at);
+              const size_t c1 = cost(t, g0, n);
+              if (c1 < c0) {
+                gained += c0 - c1;
+                c0 = c1;
+                continue;
+              }
+              flip(at);
+            }
+            const int span = hi[at] - lo[at];
+            if (span < 2) continue;
+            for (int k = 0; k < kTries; ++k) {
+              const size_t t2 = static_cast<size_t>(lo[at]) + next() % static_cast<uint64_t>(span);
+              if (t2 == t) continue;
+              const size_t at2 = t2 * lanes + g0 + i;
+              const size_t before = c0 + cost(t2, g0, n);
+              trade(at, at2);
+              const size_t c1 = cost(t, g0, n), after = c1 + cost(t2, g0, n);
+              if (after < before) {
+                gained += before - after;
+                c0 = c1;
+                break;
+              }
+              trade(at, at2);
+            }
+          }
+        }
+      }
+      if (gained == 0) break;
+    }
+  };
+  for (const Pass& p : s.fwd) refine_pass(p, true);
+  for (const Pass& p : s.rev) refine_pass(p, false);
+}
+
 double emulate_schedule(const Potential& pot, const Schedule& s, std::vector<double>& V) {
   V.resize(s.v_size, 0.0);
   for (int k : s.zero_list) V[s.v_m + k] = 0.0;

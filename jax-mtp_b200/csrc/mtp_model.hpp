@@ -116,6 +116,15 @@ struct Schedule {
 // write-before-read order, or exceeds index limits.
 bool build_schedule(const Potential& pot, int lanes, Schedule& out, std::string& err, int width = 4);
 
+// Local search over a built schedule against shared-memory bank conflicts:
+// an entry whose bank key sets a gather's wavefront count trades steps with
+// another entry of the same job (the flush stays at the job's last step), or
+// in a forward pass its two operands trade places, whenever that lowers the
+// wavefronts of both steps (bank model of build_schedule's `width`).  The
+// sums are unchanged up to their order; candidates come from a fixed-seed
+// generator, so the result is a pure function of the schedule.
+void refine_schedule(Schedule& s);
+
 // Execute the schedule for one atom on the host (bit-for-bit the device
 // arithmetic order, in double): V must have v_size entries with basic moments
 // in V[v_m .. v_m + B) set.  Fills moments, adjoints (seeded with moment

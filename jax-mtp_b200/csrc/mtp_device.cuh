@@ -753,12 +753,19 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
       __syncthreads();
     }
     // ---- N2: basic moments m[(mu, a, b, c)] of every atom of the block ------
-    // tasks (atom, monomial); monomials are sorted by degree, so the tasks of a
-    // warp share one radial-function count (the warp's largest is used)
-    for (int t0 = 0; t0 < A * P; t0 += NT) {
-      const int t = t0 + tid;
-      const bool act = t < A * P;
-      const int a = act ? t / P : 0, p = act ? t - a * P : 0;
+    // tasks (atom, monomial), most radial functions first: monomials are
+    // sorted by degree (descending), so monomial P-1-j has the j-th most.  A
+    // warp takes 32 consecutive monomials of one atom (one radial-function
+    // count and one neighbour list per warp; the warp's largest count is
+    // used), warp slots go round-robin over the atoms, and odd rounds run the
+    // slots in reverse (snake), so each thread's rounds add up to about the
+    // same cost and the last, partial round gets the cheapest monomials.
+    const int P32 = (P + 31) & ~31;
+    for (int t0 = 0; t0 < A * P32; t0 += NT) {
+      const int pos = t0 + (((t0 / NT) & 1) ? NT - 1 - tid : tid);
+      const int blk = pos >> 5, j = (blk / A) * 32 + (pos & 31);
+      const bool act = pos < A * P32 && j < P;
+      const int a = act ? blk % A : 0, p = act ? P - 1 - j : 0;
       const int4 abc = __ldg(reinterpret_cast<const int4*>(md.mono_abc) + p);
       int nv = 0;
 #pragma unroll

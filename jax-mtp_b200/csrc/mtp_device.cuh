@@ -383,30 +383,33 @@ __device__ __forceinline__ void n3_sums(const T* __restrict__ dmt, int D,
   }
 }
 
-// Force phase on level-structured bases.  Lanes take the block's kept
-// neighbours (item j = 32 c + lane over the A atoms' lists in turn), warps
-// take disjoint sets of monomial pairs (Schedule::n3_pairs, at most 32 per
-// warp; each lane holds one pair word and the warp shuffles it out), so all
-// lanes of a warp read the same adjoint row at every step (one shared-memory
-// wavefront per gather; the A atoms' values of a slot are adjacent) and no
-// lane reduces with its neighbours.  Per item and pair: the Horner chain in
-// u_z over steps k = 0 .. top with the radial functions mu <= k / 2, then the
-// powers of u_x and u_y; the warps' partial sums (G, S) meet in P
-// ([4][warps][32]) and warp 0 adds them in warp order (deterministic) and
-// writes the slot gradients.
+// Force phase on level-structured bases.  The warps form groups of GW =
+// min(warps, kN3GroupWarps); group g takes the chunks of 32 kept neighbours
+// c = g, g + groups, ... (item j = 32 c + lane over the A atoms' lists in
+// turn), and the warps of a group take disjoint sets of monomial pairs
+// (Schedule::n3_pairs, at most 32 per warp; each lane holds one pair word and
+// the warp shuffles it out), so all lanes of a warp read the same adjoint row
+// at every step (one shared-memory wavefront per gather; the A atoms' values
+// of a slot are adjacent) and no lane reduces with its neighbours.  Per item
+// and pair: the Horner chain in u_z over steps k = 0 .. top with the radial
+// functions mu <= k / 2, then the powers of u_x and u_y; the group's partial
+// sums (G, S) meet in P ([4][warps][32]) and its first warp adds them in warp
+// order (deterministic) and writes the slot gradients.
 template <typename T, int A, int R>
 __device__ __forceinline__ void n3_transposed(const DevModel& md, const DevIO& io, const SmemLayout& L,
                                               unsigned char* smem, const T* __restrict__ V,
                                               const int (&nv_a)[A], int base, int tid, int NT, T* __restrict__ P) {
   const int w = tid >> 5, lane = tid & 31, NW = NT >> 5;
+  const int GW = min(NW, kN3GroupWarps), g = w / GW, wg = w - g * GW, NG = NW / GW;
   const int D1 = md.D + 1, pws = L.pws, n_pad = io.n_pad;
-  const int p0 = __ldg(md.n3_off + w), np = __ldg(md.n3_off + w + 1) - p0;
+  const int p0 = __ldg(md.n3_off + wg), np = __ldg(md.n3_off + wg + 1) - p0;
   const int myword = lane < np ? __ldg(md.n3_pairs + p0 + lane) : 0;
   int J = 0;
 #pragma unroll
   for (int a = 0; a < A; ++a) J += nv_a[a];
-  for (int c0 = 0; c0 < J; c0 += 32) {
-    const int j = c0 + lane;
+  // every group runs the same number of rounds (the block barriers match)
+  for (int c0 = 0; c0 < J; c0 += 32 * NG) {
+    const int j = c0 + 32 * g + lane;
     const bool act = j < J;
     int a = 0, q = act ? j : 0;
 #pragma unroll
@@ -466,9 +469,9 @@ __device__ __forceinline__ void n3_transposed(const DevModel& md, const DevIO& i
     P[(2 * NW + w) * 32 + lane] = Gz;
     P[(3 * NW + w) * 32 + lane] = Ss;
     __syncthreads();
-    if (w == 0 && act) {
+    if (wg == 0 && act) {
       T gx_ = T(0), gy_ = T(0), gz_ = T(0), s_ = T(0);
-      for (int ww = 0; ww < NW; ++ww) {
+      for (int ww = w; ww < w + GW; ++ww) {
         gx_ += P[(0 * NW + ww) * 32 + lane];
         gy_ += P[(1 * NW + ww) * 32 + lane];
         gz_ += P[(2 * NW + ww) * 32 + lane];

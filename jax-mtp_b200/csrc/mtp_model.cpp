@@ -574,7 +574,7 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
         pairs.push_back({a | (b << 4) | (top << 8) | (base << 12), cost});
         base += ((top + 2) * (top + 2)) / 4;
       }
-    const int warps = lanes / 32;
+    const int warps = std::min(lanes / 32, kN3GroupWarps);
     std::vector<int> order(pairs.size());
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return pairs[x].cost > pairs[y].cost; });

@@ -35,7 +35,8 @@ constexpr int kMaxR = 8;       // radial functions supported by the kernels
 constexpr int kMaxK = 16;      // Chebyshev terms supported by the kernels
 constexpr int kMaxDegree = 12; // monomial degree supported by the kernels
 constexpr int kMaxPasses = 16;
-constexpr int kStepAlign = 4;   // pass steps are a multiple of this; as many no-op rows end the program
+constexpr int kStepAlign = 4;
+constexpr int kN3GroupWarps = 8;  // warps that share one neighbour chunk in the force phase   // pass steps are a multiple of this; as many no-op rows end the program
 
 struct Potential {
   std::string version, potential_name, potential_tag, radial_basis_type;
@@ -99,10 +100,12 @@ struct Schedule {
   bool tri = false;
   // dE/dm of moment k lives at v_dm + dm_pos[k] (a permutation of [0, M))
   std::vector<int> dm_pos;
-  // Force phase on level-structured bases: warp w of the block takes the
-  // monomial pairs n3_pairs[n3_off[w] .. n3_off[w + 1]) (at most 32, balanced
-  // by chain cost), each one word a | b << 4 | top << 8 | chain base << 12
-  // (top = D - a - b; chain base = the pair's first adjoint position).
+  // Force phase on level-structured bases: the block's warps form groups of
+  // min(lanes / 32, kN3GroupWarps) that take neighbour chunks in turn, and
+  // warp w of a group takes the monomial pairs n3_pairs[n3_off[w] ..
+  // n3_off[w + 1]) (at most 32, balanced by chain cost), each one word
+  // a | b << 4 | top << 8 | chain base << 12 (top = D - a - b; chain base =
+  // the pair's first adjoint position).
   std::vector<int> n3_pairs, n3_off;
   std::vector<int> zero_list;   // non-basic moments never written (must read as 0)
   std::vector<Pass> fwd, rev;   // passes in execution order

@@ -35,6 +35,8 @@ struct DeviceSchedule {
   uint2* d_entries = nullptr;
   int* d_n3_pairs = nullptr;   // Schedule::n3_pairs / n3_off (level-structured bases)
   int* d_n3_off = nullptr;
+  int* d_n3_pairs_half = nullptr;   // the same for the FP64 kernel's half-width groups
+  int* d_n3_off_half = nullptr;
   int* d_warp_steps = nullptr;  // [forward passes, reverse passes][lanes / 32] (Pass::wsteps)
 };
 
@@ -186,6 +188,8 @@ DevModel make_model(mtp_handle* h, const DeviceSchedule& ds) {
   md.dm_pos = h->d_dm_pos;
   md.n3_pairs = ds.d_n3_pairs;
   md.n3_off = ds.d_n3_off;
+  md.n3_pairs_half = ds.d_n3_pairs_half;
+  md.n3_off_half = ds.d_n3_off_half;
   md.warp_steps = ds.d_warp_steps;
   md.Q = s.Q;
   md.npairs = s.npairs;
@@ -268,6 +272,12 @@ int get_schedule(mtp_handle* h, int lanes, int width, DeviceSchedule** out, bool
       MTP_CUDA(h, cudaMemcpy(ds.d_n3_pairs, np.data(), np.size() * sizeof(int), cudaMemcpyHostToDevice));
       MTP_CUDA(h, dalloc(&ds.d_n3_off, no.size()));
       MTP_CUDA(h, cudaMemcpy(ds.d_n3_off, no.data(), no.size() * sizeof(int), cudaMemcpyHostToDevice));
+      const auto& nph = ds.sched.n3_pairs_half;
+      const auto& noh = ds.sched.n3_off_half;
+      MTP_CUDA(h, dalloc(&ds.d_n3_pairs_half, nph.size()));
+      MTP_CUDA(h, cudaMemcpy(ds.d_n3_pairs_half, nph.data(), nph.size() * sizeof(int), cudaMemcpyHostToDevice));
+      MTP_CUDA(h, dalloc(&ds.d_n3_off_half, noh.size()));
+      MTP_CUDA(h, cudaMemcpy(ds.d_n3_off_half, noh.data(), noh.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
   }
   *out = &ds;
@@ -299,6 +309,8 @@ void free_handle(mtp_handle* h) {
     F(kv.second.d_entries);
     F(kv.second.d_n3_pairs);
     F(kv.second.d_n3_off);
+    F(kv.second.d_n3_pairs_half);
+    F(kv.second.d_n3_off_half);
     F(kv.second.d_warp_steps);
   }
   F(h->d_radial); F(h->d_species); F(h->d_theta); F(h->d_seed_val);

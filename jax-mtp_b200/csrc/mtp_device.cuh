@@ -72,6 +72,8 @@ struct DevModel {
   const int* dm_pos;        // [M] adjoint position of each moment (Schedule::dm_pos)
   const int* n3_pairs;      // Schedule::n3_pairs / n3_off (level-structured bases)
   const int* n3_off;
+  const int* n3_pairs_half;  // Schedule::n3_pairs_half / n3_off_half (the FP64 kernel)
+  const int* n3_off_half;
   int nmu[kMaxDegree + 1];  // radial functions with a basic moment of each degree
   int v_m, v_dm, v_zero, v_one, v_size;
   double scaling, rmin, rmax;
@@ -400,10 +402,15 @@ __device__ __forceinline__ void n3_transposed(const DevModel& md, const DevIO& i
                                               unsigned char* smem, const T* __restrict__ V,
                                               const int (&nv_a)[A], int base, int tid, int NT, T* __restrict__ P) {
   const int w = tid >> 5, lane = tid & 31, NW = NT >> 5;
-  const int GW = min(NW, kN3GroupWarps), g = w / GW, wg = w - g * GW, NG = NW / GW;
+  // FP64 runs groups of half the width (fewer, shorter rounds for its fewer
+  // atoms per block; measured faster there, slower in FP32)
+  constexpr bool kHalf = sizeof(T) == 8;
+  const int* n3_off = kHalf ? md.n3_off_half : md.n3_off;
+  const int* n3_pairs = kHalf ? md.n3_pairs_half : md.n3_pairs;
+  const int GW = min(NW, kHalf ? kN3GroupWarps / 2 : kN3GroupWarps), g = w / GW, wg = w - g * GW, NG = NW / GW;
   const int D1 = md.D + 1, pws = L.pws, n_pad = io.n_pad;
-  const int p0 = __ldg(md.n3_off + wg), np = __ldg(md.n3_off + wg + 1) - p0;
-  const int myword = lane < np ? __ldg(md.n3_pairs + p0 + lane) : 0;
+  const int p0 = __ldg(n3_off + wg), np = __ldg(n3_off + wg + 1) - p0;
+  const int myword = lane < np ? __ldg(n3_pairs + p0 + lane) : 0;
   int J = 0;
 #pragma unroll
   for (int a = 0; a < A; ++a) J += nv_a[a];
@@ -512,25 +519,16 @@ __device__ __forceinline__ void moment_task(const T* __restrict__ sF, const T* _
   }
 }
 
-// Deterministic block sums of A doubles per thread (valid in thread 0).
+// Per-warp sums of A doubles per thread: lane 0 of warp w writes atom a's
+// sum to red[a * warps + w] (summed later in warp order: deterministic).
 template <int A>
-__device__ __forceinline__ void block_sum(double (&v)[A], double* red) {
+__device__ __forceinline__ void warp_partials(double (&v)[A], double* red) {
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
 #pragma unroll
   for (int a = 0; a < A; ++a) {
     for (int o = 16; o > 0; o >>= 1) v[a] += __shfl_xor_sync(0xffffffffu, v[a], o);
     if (l == 0) red[a * nw + w] = v[a];
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int a = 0; a < A; ++a) {
-      double s = 0.0;
-      for (int i = 0; i < nw; ++i) s += red[a * nw + i];
-      v[a] = s;
-    }
-  }
-  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -618,11 +616,19 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
       nv_a[a] = 0;
     }
     // tasks (atom, slot) with each atom's slots padded to whole warps, so a
-    // warp's ballot covers one atom; all atoms of the block in one sweep
+    // warp's ballot covers one atom.  In FP64, when the block has twice as
+    // many threads as tasks, every task has two threads (role 0: tid < NV,
+    // role 1: the thread NV above it): both load and test the slot (the same
+    // ballot), role 0 stores the direction and the radial functions, role 1
+    // the powers (measured faster in FP64, not in FP32)
     const int S32 = (io.nbr_stride + 31) & ~31;
-    for (int v0 = 0; v0 < A * S32; v0 += NT) {
-      const int v = v0 + tid;
-      const int a = v < A * S32 ? v / S32 : A;
+    const int NV = A * S32;
+    const bool split = sizeof(T) == 8 && 2 * NV <= NT;
+    const int span = split ? NV : NT;   // tasks per sweep
+    const int role = split ? (tid < NV ? 0 : tid < 2 * NV ? 1 : 2) : 0;
+    for (int v0 = 0; v0 < NV; v0 += span) {
+      const int v = v0 + (split ? tid - role * NV : tid);
+      const int a = (role < 2 && v < NV) ? v / S32 : A;
       const int s = v - a * S32;
       int it = 0, cnt = 0;
 #pragma unroll
@@ -654,7 +660,7 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
           d = dev_sqrt(r2);
           valid = (jt >= 0) && (r2 > T(0)) && (d < rmax);
         }
-        if (!valid) {
+        if (!valid && role == 0) {
           grow[3 * s] = 0.0;
           grow[3 * s + 1] = 0.0;
           grow[3 * s + 2] = 0.0;
@@ -662,13 +668,14 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
       }
       const unsigned bal = __ballot_sync(0xffffffffu, valid);
       const int w = tid >> 5, l = tid & 31, nw = NT >> 5;
-      if (l == 0) sCnt[w] = __popc(bal);
+      const int wt = w - role * (NV >> 5);   // the role-0 warp of these tasks
+      if (l == 0 && role == 0) sCnt[w] = __popc(bal);
       __syncthreads();
       if (tid == 0) {
         // exclusive offsets of each warp within its atom's kept slots of this
         // sweep; per-atom totals after the warp counts
         int accn = 0, cur = -1;
-        for (int i = 0; i < nw; ++i) {
+        for (int i = 0; i < (span >> 5); ++i) {
           const int ai = (v0 + 32 * i) / S32;
           if (ai != cur) {
             if (cur >= 0 && cur < A) sCnt[nw + cur] = accn;
@@ -687,7 +694,7 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
 #pragma unroll
         for (int aa = 0; aa < A; ++aa)
           if (aa == a) nv = nv_a[aa];
-        const int q = nv + sCnt[w] + __popc(bal & ((1u << l) - 1u));
+        const int q = nv + sCnt[wt] + __popc(bal & ((1u << l) - 1u));
         T* sU = reinterpret_cast<T*>(smem + L.u) + static_cast<size_t>(a) * 4 * n_pad;
         T* sF = reinterpret_cast<T*>(smem + L.f) + static_cast<size_t>(a) * R * n_pad;
         T* sFp = reinterpret_cast<T*>(smem + L.fp) + static_cast<size_t>(a) * R * n_pad;
@@ -695,62 +702,66 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
         int* sSlot = reinterpret_cast<int*>(smem + L.slot) + a * n_pad;
         const T inv_d = T(1) / d;
         const T ux = rx * inv_d, uy = ry * inv_d, uz = rz * inv_d;
-        sU[4 * q] = ux;
-        sU[4 * q + 1] = uy;
-        sU[4 * q + 2] = uz;
-        sU[4 * q + 3] = d;
-        sSlot[q] = s;
-        // Chebyshev T_n(x) and dT_n/dx by their recurrences, folded into
-        // sum_n c[t_i, t_j, mu, n] T_n for every mu as the terms appear
-        const T x = (T(2) * d - rsum) * inv_range;
-        const T dxdd = T(2) * inv_range;
-        const T* c = sRad + (static_cast<size_t>(it) * S + jt) * R * K;
-        T bas[kMaxR], dbas[kMaxR];
+        if (role == 0) {
+          sU[4 * q] = ux;
+          sU[4 * q + 1] = uy;
+          sU[4 * q + 2] = uz;
+          sU[4 * q + 3] = d;
+          sSlot[q] = s;
+          // Chebyshev T_n(x) and dT_n/dx by their recurrences, folded into
+          // sum_n c[t_i, t_j, mu, n] T_n for every mu as the terms appear
+          const T x = (T(2) * d - rsum) * inv_range;
+          const T dxdd = T(2) * inv_range;
+          const T* c = sRad + (static_cast<size_t>(it) * S + jt) * R * K;
+          T bas[kMaxR], dbas[kMaxR];
 #pragma unroll
-        for (int mu = 0; mu < kMaxR; ++mu) {
-          bas[mu] = mu < R ? c[mu * K] : T(0);   // T_0 = 1, T_0' = 0
-          dbas[mu] = T(0);
-        }
-        T t_prev = T(1), t_cur = x, dt_prev = T(0), dt_cur = T(1);
-        for (int n = 1; n < K; ++n) {
+          for (int mu = 0; mu < kMaxR; ++mu) {
+            bas[mu] = mu < R ? c[mu * K] : T(0);   // T_0 = 1, T_0' = 0
+            dbas[mu] = T(0);
+          }
+          T t_prev = T(1), t_cur = x, dt_prev = T(0), dt_cur = T(1);
+          for (int n = 1; n < K; ++n) {
+#pragma unroll
+            for (int mu = 0; mu < kMaxR; ++mu) {
+              if (mu < R) {
+                bas[mu] = dev_fma(c[mu * K + n], t_cur, bas[mu]);
+                dbas[mu] = dev_fma(c[mu * K + n], dt_cur, dbas[mu]);
+              }
+            }
+            const T t_next = T(2) * x * t_cur - t_prev;
+            const T dt_next = T(2) * t_cur + T(2) * x * dt_cur - dt_prev;
+            t_prev = t_cur;
+            t_cur = t_next;
+            dt_prev = dt_cur;
+            dt_cur = dt_next;
+          }
+          const T gap = rmax - d;
+          const T smooth = gap * gap;
 #pragma unroll
           for (int mu = 0; mu < kMaxR; ++mu) {
             if (mu < R) {
-              bas[mu] = dev_fma(c[mu * K + n], t_cur, bas[mu]);
-              dbas[mu] = dev_fma(c[mu * K + n], dt_cur, dbas[mu]);
+              sF[q * R + mu] = scal * smooth * bas[mu];
+              sFp[q * R + mu] = scal * (T(-2) * gap * bas[mu] + smooth * dbas[mu] * dxdd);
             }
           }
-          const T t_next = T(2) * x * t_cur - t_prev;
-          const T dt_next = T(2) * t_cur + T(2) * x * dt_cur - dt_prev;
-          t_prev = t_cur;
-          t_cur = t_next;
-          dt_prev = dt_cur;
-          dt_cur = dt_next;
         }
-        const T gap = rmax - d;
-        const T smooth = gap * gap;
-#pragma unroll
-        for (int mu = 0; mu < kMaxR; ++mu) {
-          if (mu < R) {
-            sF[q * R + mu] = scal * smooth * bas[mu];
-            sFp[q * R + mu] = scal * (T(-2) * gap * bas[mu] + smooth * dbas[mu] * dxdd);
+        if (role == 1 || !split) {
+          T* pw = sPw + q * pws;
+          T px = T(1), py = T(1), pz = T(1);
+          for (int e = 0; e < D1; ++e) {
+            pw[e] = px;
+            pw[D1 + e] = py;
+            pw[2 * D1 + e] = pz;
+            px *= ux;
+            py *= uy;
+            pz *= uz;
           }
-        }
-        T* pw = sPw + q * pws;
-        T px = T(1), py = T(1), pz = T(1);
-        for (int e = 0; e < D1; ++e) {
-          pw[e] = px;
-          pw[D1 + e] = py;
-          pw[2 * D1 + e] = pz;
-          px *= ux;
-          py *= uy;
-          pz *= uz;
         }
       }
       // atoms touched by this sweep add its kept count
 #pragma unroll
       for (int aa = 0; aa < A; ++aa) {
-        const int first = v0 / S32, last = (v0 + NT - 1) / S32;
+        const int first = v0 / S32, last = (v0 + span - 1) / S32;
         if (aa >= first && aa <= last) nv_a[aa] += sCnt[nw + aa];
       }
       __syncthreads();
@@ -824,17 +835,9 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
 #pragma unroll
         for (int a = 0; a < A; ++a) ep[a] = fma(th, static_cast<double>(V[k * A + a]), ep[a]);
       }
-      block_sum<A>(ep, sRed);
-      if (tid == 0) {
-#pragma unroll
-        for (int a = 0; a < A; ++a) {
-          if (base + a < io.natoms) {
-            const double e = __ldg(md.species + it_a[a]) + ep[a];
-            io.site_energy[base + a] = e;
-            if (!isfinite(e)) atomicOr(io.err, kErrNonFinite);
-          }
-        }
-      }
+      // warp sums now; the block sum waits for the reverse passes' barriers
+      // (no barrier of its own on the critical path)
+      warp_partials<A>(ep, sRed);
     }
 
     // ---- R: reverse passes (dE/dm) ---------------------------------------
@@ -842,6 +845,19 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
       run_pass_n<T, A, kVGlobal>(md.entries + md.rev[ps].offset,
                                  __shfl_sync(0xFFFFFFFFu, my_wsteps, md.nfwd + ps), NT, tid, V);
       __syncthreads();
+    }
+
+    // site energies: thread a adds atom a's warp sums in warp order
+    if (md.nrev == 0) __syncthreads();
+#pragma unroll
+    for (int a = 0; a < A; ++a) {
+      if (tid == a && base + a < io.natoms) {
+        double ep = 0.0;
+        for (int i = 0; i < (NT >> 5); ++i) ep += sRed[a * (NT >> 5) + i];
+        const double e = __ldg(md.species + it_a[a]) + ep;
+        io.site_energy[base + a] = e;
+        if (!isfinite(e)) atomicOr(io.err, kErrNonFinite);
+      }
     }
 
     // ---- N3: dE_i/dr_ij per kept neighbour -------------------------------

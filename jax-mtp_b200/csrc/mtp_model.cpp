@@ -574,24 +574,30 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
         pairs.push_back({a | (b << 4) | (top << 8) | (base << 12), cost});
         base += ((top + 2) * (top + 2)) / 4;
       }
-    const int warps = std::min(lanes / 32, kN3GroupWarps);
     std::vector<int> order(pairs.size());
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return pairs[x].cost > pairs[y].cost; });
-    std::vector<std::vector<int>> wl(warps);
-    std::vector<long> load(warps, 0);
-    for (int i : order) {
-      int w = 0;
-      for (int v = 1; v < warps; ++v)
-        if (load[v] < load[w] || (load[v] == load[w] && wl[v].size() < wl[w].size())) w = v;
-      wl[w].push_back(pairs[i].word);
-      load[w] += pairs[i].cost;
-    }
-    s.n3_off.assign(1, 0);
-    for (int w = 0; w < warps; ++w) {
-      if (wl[w].size() > 32) s.tri = false;    // one pair per lane at most
-      s.n3_pairs.insert(s.n3_pairs.end(), wl[w].begin(), wl[w].end());
-      s.n3_off.push_back(static_cast<int>(s.n3_pairs.size()));
+    // one list per group width (kN3GroupWarps: the FP32 kernel; half of it:
+    // the FP64 kernel)
+    for (int gi = 0; gi < 2; ++gi) {
+      const int warps = std::min(lanes / 32, gi == 0 ? kN3GroupWarps : kN3GroupWarps / 2);
+      std::vector<std::vector<int>> wl(warps);
+      std::vector<long> load(warps, 0);
+      for (int i : order) {
+        int w = 0;
+        for (int v = 1; v < warps; ++v)
+          if (load[v] < load[w] || (load[v] == load[w] && wl[v].size() < wl[w].size())) w = v;
+        wl[w].push_back(pairs[i].word);
+        load[w] += pairs[i].cost;
+      }
+      std::vector<int>& np = gi == 0 ? s.n3_pairs : s.n3_pairs_half;
+      std::vector<int>& no = gi == 0 ? s.n3_off : s.n3_off_half;
+      no.assign(1, 0);
+      for (int w = 0; w < warps; ++w) {
+        if (wl[w].size() > 32) s.tri = false;    // one pair per lane at most
+        np.insert(np.end(), wl[w].begin(), wl[w].end());
+        no.push_back(static_cast<int>(np.size()));
+      }
     }
     if (base >= (1 << 20) || s.D > 15) s.tri = false;
   }

@@ -36,7 +36,7 @@ constexpr int kMaxK = 16;      // Chebyshev terms supported by the kernels
 constexpr int kMaxDegree = 12; // monomial degree supported by the kernels
 constexpr int kMaxPasses = 16;
 constexpr int kStepAlign = 4;
-constexpr int kN3GroupWarps = 8;  // warps that share one neighbour chunk in the force phase   // pass steps are a multiple of this; as many no-op rows end the program
+constexpr int kN3GroupWarps = 8;  // warps that share one neighbour chunk in the FP32 force phase (half in FP64)   // pass steps are a multiple of this; as many no-op rows end the program
 
 struct Potential {
   std::string version, potential_name, potential_tag, radial_basis_type;
@@ -101,12 +101,13 @@ struct Schedule {
   // dE/dm of moment k lives at v_dm + dm_pos[k] (a permutation of [0, M))
   std::vector<int> dm_pos;
   // Force phase on level-structured bases: the block's warps form groups of
-  // min(lanes / 32, kN3GroupWarps) that take neighbour chunks in turn, and
-  // warp w of a group takes the monomial pairs n3_pairs[n3_off[w] ..
-  // n3_off[w + 1]) (at most 32, balanced by chain cost), each one word
-  // a | b << 4 | top << 8 | chain base << 12 (top = D - a - b; chain base =
-  // the pair's first adjoint position).
-  std::vector<int> n3_pairs, n3_off;
+  // min(lanes / 32, kN3GroupWarps) (FP32 kernel; n3_*_half: of half that,
+  // FP64 kernel) that take neighbour chunks in turn, and warp w of a group
+  // takes the monomial pairs n3_pairs[n3_off[w] .. n3_off[w + 1]) (at most
+  // 32, balanced by chain cost), each one word a | b << 4 | top << 8 |
+  // chain base << 12 (top = D - a - b; chain base = the pair's first
+  // adjoint position).
+  std::vector<int> n3_pairs, n3_off, n3_pairs_half, n3_off_half;
   std::vector<int> zero_list;   // non-basic moments never written (must read as 0)
   std::vector<Pass> fwd, rev;   // passes in execution order
   std::vector<uint32_t> entries;  // pairs (x, y) per entry: 2 words; kStepAlign no-op rows at the end

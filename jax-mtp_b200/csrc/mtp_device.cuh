@@ -34,6 +34,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "mtp_model.hpp"
 
 namespace mtp {
@@ -97,6 +99,12 @@ struct DevIO {
 // Lane-program entries requested ahead of use (registers), per thread.
 constexpr int kPrefetch = kStepAlign;
 
+// Radial-function values the basic-moment phase reads with one load: four
+// in FP32 (16 bytes; rows padded to match), one in FP64 (vector loads were
+// measured slower there).
+template <typename T>
+constexpr int kRadVec = sizeof(T) == 4 ? 4 : 1;
+
 // Shared-memory carve of the evaluation kernel for A atoms per block: the
 // value space is interleaved [slot][atom] so one vector access serves all A
 // atoms; neighbour staging is kept per atom.  The dense dE/dm table of the
@@ -105,6 +113,7 @@ constexpr int kPrefetch = kStepAlign;
 // space in global memory, or when it does not fit, it gets its own region.
 struct SmemLayout {
   int pws;        // stride of a power row (3 (D+1), rounded up to odd)
+  int rs;         // stride of a radial-function row (R rounded up to kRadVec)
   bool dmt_in_v;  // dense table in the moment half of the value space
   bool n3p_in_v;  // force-phase partial sums in the moment half of the value space
   size_t v, rad, u, f, fp, pw, slot, dmt, n3p, red, cnt, total;
@@ -135,8 +144,9 @@ __host__ __device__ inline SmemLayout smem_layout(int v_size, int M, int S, int 
   L.v = take(sizeof(T) * v_size * A);
   L.rad = take(sizeof(T) * S * S * R * K);
   L.u = take(sizeof(T) * 4 * n_pad * A);
-  L.f = take(sizeof(T) * R * n_pad * A);
-  L.fp = take(sizeof(T) * R * n_pad * A);
+  L.rs = (R + kRadVec<T> - 1) / kRadVec<T> * kRadVec<T>;
+  L.f = take(sizeof(T) * L.rs * n_pad * A);
+  L.fp = take(sizeof(T) * L.rs * n_pad * A);
   L.pw = take(sizeof(T) * L.pws * n_pad * A);
   L.slot = take(sizeof(int) * n_pad * A);
   L.dmt = L.dmt_in_v ? L.v : take(sizeof(T) * R * Q * A);
@@ -425,8 +435,8 @@ __device__ __forceinline__ void n3_transposed(const DevModel& md, const DevIO& i
         q -= nv_a[aa];
         a = aa + 1;
       }
-    const T* sF = reinterpret_cast<const T*>(smem + L.f) + (static_cast<size_t>(a) * n_pad + q) * R;
-    const T* sFp = reinterpret_cast<const T*>(smem + L.fp) + (static_cast<size_t>(a) * n_pad + q) * R;
+    const T* sF = reinterpret_cast<const T*>(smem + L.f) + (static_cast<size_t>(a) * n_pad + q) * L.rs;
+    const T* sFp = reinterpret_cast<const T*>(smem + L.fp) + (static_cast<size_t>(a) * n_pad + q) * L.rs;
     const T* sU = reinterpret_cast<const T*>(smem + L.u) + (static_cast<size_t>(a) * n_pad + q) * 4;
     const T* pw = reinterpret_cast<const T*>(smem + L.pw) + (static_cast<size_t>(a) * n_pad + q) * pws;
     T f[R], fp[R];
@@ -505,15 +515,20 @@ __device__ __forceinline__ void n3_transposed(const DevModel& md, const DevIO& i
 }
 
 // Basic moments of one (atom, monomial) task for NM radial functions:
-// acc[mu] = sum_q f_mu(d_q) u_x^a u_y^b u_z^c over the kept neighbours.
+// acc[mu] = sum_q f_mu(d_q) u_x^a u_y^b u_z^c over the kept neighbours.  The
+// radial rows (stride rs) are read kRadVec values per load.
 template <typename T, int NM>
-__device__ __forceinline__ void moment_task(const T* __restrict__ sF, const T* __restrict__ sPw, int R, int pws, int D1,
+__device__ __forceinline__ void moment_task(const T* __restrict__ sF, const T* __restrict__ sPw, int rs, int pws, int D1,
                                             int nv, int ea, int eb, int ec, T (&acc)[kMaxR]) {
+  constexpr int VW = kRadVec<T>, NV = (NM + VW - 1) / VW;
+  using V4 = typename std::conditional<sizeof(T) == 4, float4, double>::type;
 #pragma unroll 4
   for (int q = 0; q < nv; ++q) {
     const T* pw = sPw + q * pws;
     const T mono = pw[ea] * pw[D1 + eb] * pw[2 * D1 + ec];
-    const T* f = sF + q * R;
+    T f[NV * VW];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) *reinterpret_cast<V4*>(f + v * VW) = reinterpret_cast<const V4*>(sF + q * rs)[v];
 #pragma unroll
     for (int mu = 0; mu < NM; ++mu) acc[mu] = dev_fma(f[mu], mono, acc[mu]);
   }
@@ -696,8 +711,8 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
           if (aa == a) nv = nv_a[aa];
         const int q = nv + sCnt[wt] + __popc(bal & ((1u << l) - 1u));
         T* sU = reinterpret_cast<T*>(smem + L.u) + static_cast<size_t>(a) * 4 * n_pad;
-        T* sF = reinterpret_cast<T*>(smem + L.f) + static_cast<size_t>(a) * R * n_pad;
-        T* sFp = reinterpret_cast<T*>(smem + L.fp) + static_cast<size_t>(a) * R * n_pad;
+        T* sF = reinterpret_cast<T*>(smem + L.f) + static_cast<size_t>(a) * L.rs * n_pad;
+        T* sFp = reinterpret_cast<T*>(smem + L.fp) + static_cast<size_t>(a) * L.rs * n_pad;
         T* sPw = reinterpret_cast<T*>(smem + L.pw) + static_cast<size_t>(a) * pws * n_pad;
         int* sSlot = reinterpret_cast<int*>(smem + L.slot) + a * n_pad;
         const T inv_d = T(1) / d;
@@ -740,8 +755,8 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
 #pragma unroll
           for (int mu = 0; mu < kMaxR; ++mu) {
             if (mu < R) {
-              sF[q * R + mu] = scal * smooth * bas[mu];
-              sFp[q * R + mu] = scal * (T(-2) * gap * bas[mu] + smooth * dbas[mu] * dxdd);
+              sF[q * L.rs + mu] = scal * smooth * bas[mu];
+              sFp[q * L.rs + mu] = scal * (T(-2) * gap * bas[mu] + smooth * dbas[mu] * dxdd);
             }
           }
         }
@@ -786,21 +801,21 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
       for (int aa = 0; aa < A; ++aa)
         if (act && aa == a) nv = nv_a[aa];
       const int nm = __reduce_max_sync(0xffffffffu, act ? md.nmu[abc.w] : 0);
-      const T* sF = reinterpret_cast<const T*>(smem + L.f) + static_cast<size_t>(a) * R * n_pad;
+      const T* sF = reinterpret_cast<const T*>(smem + L.f) + static_cast<size_t>(a) * L.rs * n_pad;
       const T* sPw = reinterpret_cast<const T*>(smem + L.pw) + static_cast<size_t>(a) * pws * n_pad;
       T acc[kMaxR];
 #pragma unroll
       for (int mu = 0; mu < kMaxR; ++mu) acc[mu] = T(0);
       switch (nm) {
         case 0: break;
-        case 1: moment_task<T, 1>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
-        case 2: moment_task<T, 2>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
-        case 3: moment_task<T, 3>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
-        case 4: moment_task<T, 4>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
-        case 5: moment_task<T, 5>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
-        case 6: moment_task<T, 6>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
-        case 7: moment_task<T, 7>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
-        default: moment_task<T, 8>(sF, sPw, R, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 1: moment_task<T, 1>(sF, sPw, L.rs, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 2: moment_task<T, 2>(sF, sPw, L.rs, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 3: moment_task<T, 3>(sF, sPw, L.rs, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 4: moment_task<T, 4>(sF, sPw, L.rs, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 5: moment_task<T, 5>(sF, sPw, L.rs, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 6: moment_task<T, 6>(sF, sPw, L.rs, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        case 7: moment_task<T, 7>(sF, sPw, L.rs, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
+        default: moment_task<T, 8>(sF, sPw, L.rs, pws, D1, nv, abc.x, abc.y, abc.z, acc); break;
       }
       if (act) {
 #pragma unroll
@@ -891,8 +906,8 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
       const int atom = base + a;
       const int nv = nv_a[a];
       const T* sU = reinterpret_cast<T*>(smem + L.u) + static_cast<size_t>(a) * 4 * n_pad;
-      const T* sF = reinterpret_cast<T*>(smem + L.f) + static_cast<size_t>(a) * R * n_pad;
-      const T* sFp = reinterpret_cast<T*>(smem + L.fp) + static_cast<size_t>(a) * R * n_pad;
+      const T* sF = reinterpret_cast<T*>(smem + L.f) + static_cast<size_t>(a) * L.rs * n_pad;
+      const T* sFp = reinterpret_cast<T*>(smem + L.fp) + static_cast<size_t>(a) * L.rs * n_pad;
       const T* sPw = reinterpret_cast<T*>(smem + L.pw) + static_cast<size_t>(a) * pws * n_pad;
       const int* sSlot = reinterpret_cast<int*>(smem + L.slot) + a * n_pad;
       double* grow = io.pair_grad + static_cast<size_t>(atom < io.natoms ? atom : 0) * io.nbr_stride * 3;
@@ -918,8 +933,8 @@ __global__ void __maxnreg__((EvalRegs<T, kVGlobal, A>::value)) k_mtp_eval(DevMod
           switch (R) {
 #define MTP_N3_CASE(RR)                                                                                        \
   case RR:                                                                                                     \
-    n3_sums<T, RR, kTwoN>(dmt, md.D, md.npairs, D1, sF + q0 * R, sFp + q0 * R, sF + qb * R,         \
-                                   sFp + qb * R, two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2],         \
+    n3_sums<T, RR, kTwoN>(dmt, md.D, md.npairs, D1, sF + q0 * L.rs, sFp + q0 * L.rs, sF + qb * L.rs, \
+                                   sFp + qb * L.rs, two, sPw + q0 * pws, sPw + qb * pws, sU[4 * q0 + 2],         \
                                    sU[4 * qb + 2], sl, tpn, Ssum, Gx, Gy, Gz);                                \
     break;
             MTP_N3_CASE(1) MTP_N3_CASE(2) MTP_N3_CASE(3) MTP_N3_CASE(4)

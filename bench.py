@@ -28,6 +28,7 @@ independent replicas ("scaling": "weak").
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import math
 import os
@@ -852,11 +853,16 @@ def run_pair_call(args):
                              ("mtp_execute_potential", bridge), ("mtp_compute_positions", positions)):
                 for _ in range(5):
                     fn()
+                # buffers of earlier legs are freed now, not by a collection
+                # (cudaFreeHost of gigabytes) inside the timed calls
+                gc.collect()
+                gc.disable()
                 st0 = eng.stats()
                 t0 = time.perf_counter()
                 for _ in range(calls):
                     fn()
                 us = (time.perf_counter() - t0) / calls * 1e6
+                gc.enable()
                 st1 = eng.stats()
                 out[f"{prec}_{name}_us"] = us
                 out[f"{prec}_{name}_atom_steps_per_s"] = N / (us * 1e-6)

@@ -630,11 +630,16 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
   }
   // reverse: passes for target depth maxd..1 gather sides whose source has
   // depth >= 1; every side into a depth-0 source waits for one final pass.
+  // A source's first job in execution order stores its sum unless the slot
+  // holds a seed (a scalar moment's coefficient); later ones add to it.
+  std::vector<char> seeded(M, 0), written(M, 0);
+  for (int v : pot.mapping) seeded[v] = 1;
   auto add_side = [&](std::vector<Job>& jobs, std::map<int, int>& job_of, int src, int tgt, int other, int mult) {
     auto it = job_of.find(src);
     if (it == job_of.end()) {
       job_of[src] = static_cast<int>(jobs.size());
-      jobs.push_back(Job{static_cast<uint32_t>(s.v_dm + s.dm_pos[src]), kOpAdd, {}});
+      jobs.push_back(Job{static_cast<uint32_t>(s.v_dm + s.dm_pos[src]),
+                         (seeded[src] || written[src]) ? kOpAdd : kOpStore, {}});
       it = job_of.find(src);
     }
     jobs[it->second].sides.push_back(Side{static_cast<uint32_t>(s.v_dm + s.dm_pos[tgt]),
@@ -650,6 +655,7 @@ bool build_schedule(const Potential& pot, int lanes, Schedule& s, std::string& e
       if (depth[r[1]] >= 1) add_side(jobs, job_of, r[1], r[3], r[0], r[2]);
     }
     emit_jobs(jobs, lanes, width, false, rev, parts);
+    for (const auto& kv : job_of) written[kv.first] = 1;
   }
   {
     std::vector<Job> jobs;

@@ -3,7 +3,7 @@
 The fixtures were produced by tests/golden/make_golden.py from the reference's
 numpy modules (MLIPMomentBasis.calculate, the dense tensordot tree with
 BasisConverter's coefficient remap, and finite differences of the reference
-energy).  This pins the oracle before it is used to judge the CUDA kernels.
+energy).  This pins the oracle before it is used to check the CUDA kernels.
 """
 
 import numpy as np

@@ -1,0 +1,106 @@
+"""Basis generated from the level alone (CPU).
+
+mtp_b200.basis enumerates the reference's scalar contractions of basic moment
+tensors (moment_jax.py:116-212) and compiles them into MLIP tables.  The
+reference itself checks its enumerated basis against the MLIP template of a
+level by value (conversion.py:105-160, "they now agree perfectly"); here the
+same check is made against the templates this repository's benchmark
+potentials carry (their tables came from the reference's untrained_mtps
+templates): as sets of functions on random neighbours, both ways, at levels 16,
+20, 24 and 28 (level 28 with the template's limits mu <= 5, nu <= 10).  The
+compiled tables must reproduce the dense tensor contractions, and a generated
+potential must load in the C++ parser and run through the schedule emulator.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import potential_path
+from mtp_b200 import basis as B
+from mtp_b200.engine import parse_info, schedule_emulate
+from mtp_b200.mtp_file import read_mtp, with_random_coeffs, write_mtp
+
+TEMPLATES = {16: "cfg0_L16_S1.mtp", 20: "cfg3_L20_S2.mtp", 24: "cfg2_L24_S3.mtp", 28: "cfg4_L28_S4.mtp"}
+LIMITS = {28: dict(mu_max=5, nu_max=10)}
+
+
+def _mlip_values(pot, u, rb):
+    """Scalar functions of a potential's MLIP tables on neighbours (u, rb)."""
+    basic = np.asarray(pot.alpha_index_basic).reshape(-1, 4)
+    times = np.asarray(pot.alpha_index_times).reshape(-1, 4)
+    m = np.zeros(pot.alpha_moments_count)
+    for k, (mu, a, b, c) in enumerate(basic):
+        m[k] = (rb[mu] * u[:, 0] ** a * u[:, 1] ** b * u[:, 2] ** c).sum()
+    for i1, i2, mult, i3 in times:
+        m[i3] += mult * m[i1] * m[i2]
+    return m[np.asarray(pot.alpha_moment_mapping)]
+
+
+def _unmatched(a, b, rtol=1e-8):
+    """How many values of a have no partner in b (each partner used once)."""
+    free = np.ones(len(b), bool)
+    miss = 0
+    for x in a:
+        hit = np.flatnonzero(free & (np.abs(b - x) <= rtol * abs(x)))
+        if len(hit):
+            free[hit[0]] = False
+        else:
+            miss += 1
+    return miss
+
+
+def test_scalar_counts_of_low_levels():
+    # counts of the MLIP templates' alpha_scalar_moments for levels 2-16
+    expect = {2: 1, 4: 2, 6: 5, 8: 9, 10: 16, 12: 29, 14: 52, 16: 92}
+    for level, n in expect.items():
+        assert len(B.enumerate_scalars(level)) == n, level
+
+
+@pytest.mark.parametrize("level", sorted(TEMPLATES))
+def test_generated_basis_equals_the_template_basis(level):
+    pot = read_mtp(potential_path(TEMPLATES[level]))
+    tables = B.build_basis(level, **LIMITS.get(level, {}))
+    assert len(tables.mapping) == pot.alpha_scalar_moments
+    assert len(tables.basic) == pot.alpha_index_basic_count
+    for seed in (3, 41):
+        u, rb = B.test_inputs(tables.radial_funcs_count, seed=seed, neighbours=9)
+        ours = B.table_values(tables, u, rb)
+        theirs = _mlip_values(pot, u, rb)
+        assert _unmatched(theirs, ours) == 0 and _unmatched(ours, theirs) == 0
+
+
+def test_level_28_without_the_template_limits_adds_ten_functions():
+    # mu up to 6 and nu up to 12 (the level's own limits) add 10 functions,
+    # every one with mu = 6 or nu >= 11
+    assert len(B.enumerate_scalars(28)) == 2455
+
+
+@pytest.mark.parametrize("level", [8, 12, 16, 20])
+def test_tables_reproduce_the_dense_contractions(level):
+    tables = B.build_basis(level)
+    u, rb = B.test_inputs(tables.radial_funcs_count, seed=5, neighbours=8)
+    ev = B.DenseEval(u, rb)
+    dense = np.array([float(ev.value(s)) for s in tables.scalars])
+    got = B.table_values(tables, u, rb)
+    np.testing.assert_allclose(got, dense, rtol=1e-12, atol=1e-12 * np.abs(dense).max())
+    assert tables.times[:, 2].max() <= B.MAX_MULT
+
+
+@pytest.mark.parametrize("level,lanes,width", [(16, 256, 8), (20, 512, 16)])
+def test_generated_potential_loads_and_runs_in_the_schedule(tmp_path, level, lanes, width):
+    pot = with_random_coeffs(B.template_potential(level, 2), seed=9)
+    path = tmp_path / f"gen{level}.mtp"
+    write_mtp(str(path), pot)
+    info = parse_info(str(path))
+    assert info["alpha_scalar_moments"] == pot.alpha_scalar_moments
+    rng = np.random.default_rng(2)
+    basic = rng.normal(size=pot.alpha_index_basic_count)
+    m, dm, e = schedule_emulate(str(path), lanes, basic, width)
+    # the same tables evaluated directly
+    ref = np.zeros(pot.alpha_moments_count)
+    ref[: len(basic)] = basic
+    for i1, i2, mult, i3 in pot.alpha_index_times:
+        ref[i3] += mult * ref[i1] * ref[i2]
+    np.testing.assert_allclose(m, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+    e_ref = float(np.dot(pot.moment_coeffs, ref[pot.alpha_moment_mapping]))
+    assert abs(e - e_ref) <= 1e-12 * max(1.0, abs(e_ref))

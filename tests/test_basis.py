@@ -4,24 +4,27 @@ mtp_b200.basis enumerates the reference's scalar contractions of basic moment
 tensors (moment_jax.py:116-212) and compiles them into MLIP tables.  The
 reference itself checks its enumerated basis against the MLIP template of a
 level by value (conversion.py:105-160, "they now agree perfectly"); here the
-same check is made against the templates this repository's benchmark
-potentials carry (their tables came from the reference's untrained_mtps
-templates): as sets of functions on random neighbours, both ways, at levels 16,
-20, 24 and 28 (level 28 with the template's limits mu <= 5, nu <= 10).  The
+same check is made against the reference's own data -- its dense-tree basis
+(levels 2-24) and the MLIP templates' basis (levels 2-28, 26 and 28 with the
+templates' limits mu <= 5, nu <= 10) -- as sets of values on the reference's
+test vectors, both ways, and against the tables of two benchmark potentials
+(levels 16 and 20) on random neighbours.  The
 compiled tables must reproduce the dense tensor contractions, and a generated
 potential must load in the C++ parser and run through the schedule emulator.
 """
 
+import os
+
 import numpy as np
 import pytest
 
-from conftest import potential_path
+from conftest import GOLDEN, potential_path
 from mtp_b200 import basis as B
 from mtp_b200.engine import parse_info, schedule_emulate
 from mtp_b200.mtp_file import read_mtp, with_random_coeffs, write_mtp
 
-TEMPLATES = {16: "cfg0_L16_S1.mtp", 20: "cfg3_L20_S2.mtp", 24: "cfg2_L24_S3.mtp", 28: "cfg4_L28_S4.mtp"}
-LIMITS = {28: dict(mu_max=5, nu_max=10)}
+TEMPLATES = {16: "cfg0_L16_S1.mtp", 20: "cfg3_L20_S2.mtp"}
+LIMITS = {}
 
 
 def _mlip_values(pot, u, rb):
@@ -49,14 +52,27 @@ def _unmatched(a, b, rtol=1e-8):
     return miss
 
 
-def test_scalar_counts_of_low_levels():
-    # counts of the MLIP templates' alpha_scalar_moments for levels 2-16
-    expect = {2: 1, 4: 2, 6: 5, 8: 9, 10: 16, 12: 29, 14: 52, 16: 92}
-    for level, n in expect.items():
-        assert len(B.enumerate_scalars(level)) == n, level
+@pytest.mark.parametrize("level", list(range(2, 30, 2)))
+def test_generated_basis_equals_the_reference_basis(level):
+    """known_answer_basis.npz (made by tests/golden/make_golden.py from the
+    reference's own code at its TEST_R_UNITS / TEST_RB_VALUES) holds, per
+    level, the reference's dense-tree basis (levels 2-24, from its precomputed
+    contraction lists) and the MLIP template's basis (levels 2-28).  The
+    generated basis must equal both as sets of values (levels 26 and 28 with
+    the templates' limits mu <= 5, nu <= 10)."""
+    kat = np.load(os.path.join(GOLDEN, "known_answer_basis.npz"))
+    u, rb = kat["test_r_units"], kat["test_rb_values"]
+    tables = B.build_basis(level, **({} if level < 26 else dict(mu_max=5, nu_max=10)))
+    ours = B.table_values(tables, u, rb)
+    for kind in ("tree", "mlip"):
+        key = f"L{level}_{kind}_basis"
+        if key in kat.files:
+            ref = kat[key]
+            assert len(ref) == len(ours), key
+            assert _unmatched(ref, ours) == 0 and _unmatched(ours, ref) == 0, key
 
 
-@pytest.mark.parametrize("level", sorted(TEMPLATES))
+@pytest.mark.parametrize("level", [16, 20])
 def test_generated_basis_equals_the_template_basis(level):
     pot = read_mtp(potential_path(TEMPLATES[level]))
     tables = B.build_basis(level, **LIMITS.get(level, {}))

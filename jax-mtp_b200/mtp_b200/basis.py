@@ -404,6 +404,42 @@ def template_potential(level: int, species_count: int, radial_basis_size: int = 
     return pot
 
 
+def mlip_values(pot, u: np.ndarray, rb: np.ndarray) -> np.ndarray:
+    """The scalar basis functions of a potential's MLIP tables on neighbours
+    (u, rb) (basic moments, then the products, conversion.py:39-84)."""
+    basic = np.asarray(pot.alpha_index_basic).reshape(-1, 4)
+    times = np.asarray(pot.alpha_index_times).reshape(-1, 4)
+    m = np.zeros(pot.alpha_moments_count)
+    for k, (mu, a, b, c) in enumerate(basic):
+        m[k] = (rb[mu] * u[:, 0] ** a * u[:, 1] ** b * u[:, 2] ** c).sum()
+    for i1, i2, mult, i3 in times:
+        m[i3] += mult * m[i1] * m[i2]
+    return m[np.asarray(pot.alpha_moment_mapping)]
+
+
+def remap_moment_coeffs(src, dst, rtol: float = 1e-8, seed: int = 2024) -> np.ndarray:
+    """The moment coefficients of potential src, ordered for the basis of
+    potential dst: each basis function of dst is found among src's by its value
+    on random neighbours (the reference's BasisConverter matches the same way,
+    conversion.py:112-168).  Every function of either basis must have exactly
+    one partner; otherwise ValueError."""
+    R = max(int(np.max(np.asarray(src.alpha_index_basic)[:, 0])),
+            int(np.max(np.asarray(dst.alpha_index_basic)[:, 0]))) + 1
+    u, rb = test_inputs(R, seed=seed, neighbours=11)
+    vs, vd = mlip_values(src, u, rb), mlip_values(dst, u, rb)
+    if len(vs) != len(vd):
+        raise ValueError(f"the bases differ in size: {len(vs)} and {len(vd)} functions")
+    free = np.ones(len(vs), bool)
+    out = np.empty(len(vd))
+    for i, x in enumerate(vd):
+        hit = np.flatnonzero(free & (np.abs(vs - x) <= rtol * abs(x)))
+        if len(hit) == 0:
+            raise ValueError(f"basis function {i} of the target has no partner in the source")
+        free[hit[0]] = False
+        out[i] = np.asarray(src.moment_coeffs)[hit[0]]
+    return out
+
+
 def main(argv=None) -> int:
     """python -m mtp_b200.basis LEVEL SPECIES OUT.mtp [options]: write an
     untrained potential of a level (zero coefficients)."""

@@ -27,18 +27,6 @@ TEMPLATES = {16: "cfg0_L16_S1.mtp", 20: "cfg3_L20_S2.mtp"}
 LIMITS = {}
 
 
-def _mlip_values(pot, u, rb):
-    """Scalar functions of a potential's MLIP tables on neighbours (u, rb)."""
-    basic = np.asarray(pot.alpha_index_basic).reshape(-1, 4)
-    times = np.asarray(pot.alpha_index_times).reshape(-1, 4)
-    m = np.zeros(pot.alpha_moments_count)
-    for k, (mu, a, b, c) in enumerate(basic):
-        m[k] = (rb[mu] * u[:, 0] ** a * u[:, 1] ** b * u[:, 2] ** c).sum()
-    for i1, i2, mult, i3 in times:
-        m[i3] += mult * m[i1] * m[i2]
-    return m[np.asarray(pot.alpha_moment_mapping)]
-
-
 def _unmatched(a, b, rtol=1e-8):
     """How many values of a have no partner in b (each partner used once)."""
     free = np.ones(len(b), bool)
@@ -81,7 +69,7 @@ def test_generated_basis_equals_the_template_basis(level):
     for seed in (3, 41):
         u, rb = B.test_inputs(tables.radial_funcs_count, seed=seed, neighbours=9)
         ours = B.table_values(tables, u, rb)
-        theirs = _mlip_values(pot, u, rb)
+        theirs = B.mlip_values(pot, u, rb)
         assert _unmatched(theirs, ours) == 0 and _unmatched(ours, theirs) == 0
 
 
@@ -120,3 +108,25 @@ def test_generated_potential_loads_and_runs_in_the_schedule(tmp_path, level, lan
     np.testing.assert_allclose(m, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
     e_ref = float(np.dot(pot.moment_coeffs, ref[pot.alpha_moment_mapping]))
     assert abs(e - e_ref) <= 1e-12 * max(1.0, abs(e_ref))
+
+
+def test_coefficients_move_between_bases():
+    """The level-16 benchmark potential's coefficients, remapped onto the
+    generated level-16 basis (BasisConverter's matching by value), give the
+    same potential: energies and forces of the C++ FP64 oracle agree."""
+    from mtp_b200 import synth
+    from oracle.cpu_ref import CpuMTP
+    src = read_mtp(potential_path("cfg1md_L16_S2.mtp"))
+    dst = B.template_potential(16, src.species_count, src.radial_basis_size, src.min_dist, src.max_dist)
+    dst.radial_coeffs = np.array(src.radial_coeffs, copy=True)
+    dst.species_coeffs = np.array(src.species_coeffs, copy=True)
+    dst.scaling = src.scaling
+    dst.moment_coeffs = B.remap_moment_coeffs(src, dst)
+    s = synth.lattice_structure("bcc", 2.87, (3, 3, 3))
+    s.types = (np.arange(s.natoms) % 2).astype(np.int32)
+    s.positions = s.positions + np.random.default_rng(5).normal(0.0, 0.05, s.positions.shape)
+    nd = synth.build_neighbors(s, src.max_dist)
+    a = CpuMTP(src).compute(nd.itypes, nd.rijs, nd.js, nd.jtypes, nd.counts)
+    b = CpuMTP(dst).compute(nd.itypes, nd.rijs, nd.js, nd.jtypes, nd.counts)
+    assert abs(a["energy"] - b["energy"]) <= 1e-10 * abs(a["energy"])
+    assert np.abs(a["forces"] - b["forces"]).max() <= 1e-10 * np.abs(a["forces"]).max()

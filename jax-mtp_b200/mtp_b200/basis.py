@@ -327,15 +327,9 @@ def compile_tables(level: int, scalars: Sequence[Node]) -> BasisTables:
             visit(rk)
         order.append(key)
 
-    import sys
-    limit = sys.getrecursionlimit()
-    sys.setrecursionlimit(max(limit, 100000))
-    try:
-        out_keys = [(s, ()) for s in scalars]
-        for k in out_keys:
-            visit(k)
-    finally:
-        sys.setrecursionlimit(limit)
+    out_keys = [(s, ()) for s in scalars]
+    for k in out_keys:          # recursion depth: the tree depth (at most four moments)
+        visit(k)
     # basic moments by (mu, degree, a, b), then every intermediate in order
     def mono_of(k: Key) -> Mono:
         return k[1][0] if k[1] else (0, 0, 0)
